@@ -1,0 +1,244 @@
+/*
+ * irisb200 -- C ABI of the B200 iris uniqueness hot path.
+ *
+ * The three MPC parties of worldcoin/iris-mpc run co-resident on one GPU.
+ * Each party has its own CUDA stream and memory pool; a message from one
+ * party to the next is a device-buffer handoff on that GPU instead of an NCCL
+ * send/recv.  Every entry point returns 0 on success or a negative irs_status
+ * (it never aborts); irs_last_error() describes the last failure of the
+ * calling thread.  Handles are opaque; host buffers are caller-owned; device
+ * buffers are library-owned unless a function says otherwise.  Streams are
+ * passed as void* (cudaStream_t); NULL means the party's own stream.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * worldcoin/iris-mpc).
+ */
+#ifndef IRISB200_H
+#define IRISB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum irs_status {
+  IRS_OK = 0,
+  IRS_ERR_INVALID = -1,    /* bad argument or shape */
+  IRS_ERR_CUDA = -2,       /* CUDA runtime error */
+  IRS_ERR_NOMEM = -3,      /* device allocation failed */
+  IRS_ERR_STATE = -4,      /* call out of order (e.g. dot before query upload) */
+  IRS_ERR_DEVICE = -5,     /* a kernel reported an error (bounded wait expired) */
+  IRS_ERR_OVERFLOW = -6,   /* a result list exceeded its capacity */
+};
+
+#define IRS_IRIS_CODE_LENGTH 12800 /* iris-mpc-common/src/lib.rs:15 */
+#define IRS_MASK_CODE_LENGTH 6400  /* iris-mpc-common/src/lib.rs:16 */
+#define IRS_ROTATIONS 31           /* iris-mpc-common/src/lib.rs:17 */
+#define IRS_SLOT_ROWS 32           /* query rows per query iris: 31 rotations + 1 pad row */
+#define IRS_MAX_MATCHES_LEN 256    /* iris-mpc-gpu/src/dot/distance_comparator.rs:26 */
+#define IRS_THRESHOLD_A 20316u     /* iris-mpc-gpu/src/dot/mod.rs:12 (ratio 0.345) */
+#define IRS_THRESHOLD_ANON_STATS_A 16384u /* iris-mpc-gpu/src/dot/mod.rs:14 (ratio 0.375) */
+
+/* Last error message of the calling thread ("" if none). */
+const char* irs_last_error(void);
+/* Library build string (architecture, version). */
+const char* irs_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Device manager: one GPU hosting the three parties.                        */
+/* Replaces DeviceManager::init / fork_streams / split_into_n_chunks          */
+/* (iris-mpc-gpu/src/helpers/device_manager.rs:28-157) and the NCCL ring of   */
+/* NcclComm (iris-mpc-gpu/src/helpers/comm.rs:8-270,                          */
+/* device_manager.rs:289-344): party p sends to (p+1)%3 and receives from     */
+/* (p+2)%3 through device buffers.                                            */
+/* ------------------------------------------------------------------------ */
+typedef struct irs_device_manager irs_device_manager;
+
+int irs_device_manager_init(int device, irs_device_manager** out);
+int irs_device_manager_destroy(irs_device_manager* dm);
+/* The CUDA stream of party `party` (0..2). */
+int irs_device_manager_stream(irs_device_manager* dm, int party, void** stream);
+/* Synchronise all party streams (DeviceManager::await_streams). */
+int irs_device_manager_synchronize(irs_device_manager* dm);
+/* Device error word: 0, or the code of the first bounded wait that expired. */
+int irs_device_manager_error(irs_device_manager* dm, int* code);
+int irs_device_manager_clear_error(irs_device_manager* dm);
+/* Number of SMs the persistent kernels size their grids to. */
+int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
+
+/* Plain device memory helpers for callers that stage their own buffers. */
+int irs_device_alloc(irs_device_manager* dm, size_t bytes, void** ptr);
+int irs_device_free(irs_device_manager* dm, void* ptr);
+int irs_copy_h2d(void* dst, const void* src, size_t bytes, void* stream);
+int irs_copy_d2h(void* dst, const void* src, size_t bytes, void* stream);
+int irs_stream_synchronize(void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* ShareDB: one party's dot-product engine over a device-resident share DB.   */
+/* (iris-mpc-gpu/src/dot/share_db.rs:448-1070)                               */
+/* ------------------------------------------------------------------------ */
+typedef struct irs_sharedb irs_sharedb;
+
+/* ShareDB::init (share_db.rs:467-573).  code_length: 12800 (codes) or 6400
+ * (trimmed masks).  query_length: query rows per batch (padded internally to
+ * a multiple of 64).  seed0 = this party's own ChaCha seed, seed1 = the
+ * previous party's seed; is_remote = 0 disables the zero-share mask (the
+ * reference's empty `comms`). */
+int irs_sharedb_init(irs_device_manager* dm, int peer_id, size_t max_db_length, size_t query_length,
+                     size_t code_length, const uint32_t seed0[8], const uint32_t seed1[8], int is_remote,
+                     irs_sharedb** out);
+int irs_sharedb_destroy(irs_sharedb* db);
+/* ShareDB::alloc_db (share_db.rs:575-618); the DB lives in HBM. */
+int irs_sharedb_alloc_db(irs_sharedb* db, size_t max_db_length);
+/* ShareDB::load_single_record_from_db for records first..first+n-1
+ * (share_db.rs:620-655): u16 share coefficients [n][code_length]. */
+int irs_sharedb_load_records(irs_sharedb* db, size_t first, size_t n, const uint16_t* records);
+/* ShareDB::load_single_record_from_s3 (share_db.rs:657-684): the stored i8
+ * limbs (byte - 128), [n][code_length] each. */
+int irs_sharedb_load_records_i8(irs_sharedb* db, size_t first, size_t n, const uint8_t* limb0,
+                                const uint8_t* limb1);
+/* Reads records first..first+n-1 back as u16 coefficients [n][code_length]
+ * (the inverse of load_records; CudaVec2DSlicer limb planes,
+ * iris-mpc-gpu/src/helpers/query_processor.rs:20-60). */
+int irs_sharedb_fetch_records(irs_sharedb* db, size_t first, size_t n, uint16_t* records);
+/* Number of valid records (SlicedProcessedDatabase db_lens). */
+int irs_sharedb_set_db_len(irs_sharedb* db, size_t len);
+int irs_sharedb_db_len(irs_sharedb* db, size_t* len);
+/* Fills records first..first+n-1 of the six engines (party p code/mask) with
+ * the seeded synthetic irises of the benchmark workload (device-side). */
+int irs_sharedb_synth_db(irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3], uint64_t seed,
+                         size_t first, size_t n);
+
+/* Query upload: preprocess_query + htod_transfer_query
+ * (share_db.rs:45-59; device_manager.rs:159-212), rows given as-is
+ * [n_rows][code_length] (already Lagrange-preprocessed and rotated). */
+int irs_sharedb_query_upload(irs_sharedb* db, const uint16_t* rows, size_t n_rows);
+
+/* Query slot: 32 query rows holding rotations rot_lo..rot_lo+n_rot-1 of base
+ * query `src` (rotation index 15 = centre, all_rotations(),
+ * galois_engine.rs:197-206), reported as bitmap row `query`. */
+typedef struct irs_query_slot {
+  uint32_t src;
+  uint32_t rot_lo;
+  uint32_t n_rot;
+  uint32_t query;
+} irs_query_slot;
+
+/* Uploads preprocessed base query shares [n_base][code_length] and expands
+ * the rotations on the device into 32-row slots (row 32*s + r). */
+int irs_sharedb_query_upload_slots(irs_sharedb* db, const uint16_t* base, size_t n_base,
+                                   const irs_query_slot* slots, size_t n_slots);
+/* Starts a new batch: the zero-share mask and circuit keystreams are drawn at
+ * ChaCha counter (batch_id << 40) | position (ChaChaCtx counter,
+ * iris-mpc-gpu/src/rng/chacha.rs:205-250). */
+int irs_sharedb_set_batch(irs_sharedb* db, uint64_t batch_id);
+
+/* ShareDB::dot + dot_reduce_and_multiply (share_db.rs:800-905) fused:
+ * entries [offset, offset+len) against the uploaded queries; result shares
+ * (multiplier * dot + ks_own - ks_prev mod 2^16) stay on the device.
+ * offset must be a multiple of 32. */
+int irs_sharedb_dot(irs_sharedb* db, size_t offset, size_t len, uint16_t multiplier, void* stream);
+/* The same for several engines in one launch (e.g. 3 parties x code/mask);
+ * multipliers[i] per engine; stream NULL = party 0's stream. */
+int irs_sharedb_dot_many(irs_sharedb* const* engines, const uint16_t* multipliers, int n, size_t offset,
+                         size_t len, void* stream);
+/* ShareDB::fetch_results (share_db.rs:1038-1048): the party's own result
+ * share in the reference layout [query_length][len]. */
+int irs_sharedb_fetch_results(irs_sharedb* db, uint16_t* host, size_t len);
+/* ShareDB::result_chunk_shares (share_db.rs:1050-1069): device pointer to the
+ * party's own share, layout [entry][row_stride] (entry-major).  The replicated
+ * `b` share of party p is party (p+2)%3's own share (reshare_results,
+ * share_db.rs:1004-1036, becomes this handoff). */
+int irs_sharedb_result_view(irs_sharedb* db, const uint16_t** dev, size_t* row_stride);
+
+/* ------------------------------------------------------------------------ */
+/* Circuits: the threshold protocol of the three parties.                    */
+/* (iris-mpc-gpu/src/threshold_ring/protocol.rs:433-2611)                    */
+/* ------------------------------------------------------------------------ */
+typedef struct irs_circuits irs_circuits;
+
+/* Circuits::new for the three parties (protocol.rs:463-514).
+ * seeds[p] = party p's (seed0, seed1); seed1 of party p must equal seed0 of
+ * party (p+2)%3 (the correlated-randomness ring). */
+int irs_circuits_new(irs_device_manager* dm, const uint32_t seeds[3][2][8], irs_circuits** out);
+int irs_circuits_destroy(irs_circuits* c);
+int irs_circuits_set_batch(irs_circuits* c, uint64_t batch_id);
+
+/* compare_threshold_masked_many (protocol.rs:2519-2546) on n elements
+ * (multiple of 64).  code_a[p]/mask_a[p]: party p's own u16 share (device);
+ * party p's second share is party (p+2)%3's own.  res_a[p]/res_b[p]:
+ * device u64 words (n/64) receiving party p's replicated share of the match
+ * bit (bit i of word w = element 64w + i); either may be NULL.  opened:
+ * optional device u64 words receiving the opened bits. */
+int irs_circuits_compare_threshold_masked_many(irs_circuits* c, const uint16_t* const code_a[3],
+                                               const uint16_t* const mask_a[3], size_t n, uint32_t threshold_a,
+                                               uint64_t* const res_a[3], uint64_t* const res_b[3], uint64_t* opened,
+                                               void* stream);
+/* lift_mul_sub + extract_msb with the lifted mask at zero
+ * (tests/extract_msb_mod.rs:180-215): msb of -code*2^16 - 1. */
+int irs_circuits_extract_msb_of_code(irs_circuits* c, const uint16_t* const code_a[3], size_t n,
+                                     uint64_t* const res_a[3], uint64_t* const res_b[3], uint64_t* opened,
+                                     void* stream);
+/* lift_mpc (protocol.rs:2041-2074): per party p, corr[p] receives two u16
+ * arrays of n (party p's own component of the injected carries c1, c2);
+ * sum_p mask_p - (sum corr1 << 16) - (sum corr2 << 17) = mask in Z_2^32. */
+int irs_circuits_lift_mpc(irs_circuits* c, const uint16_t* const mask_a[3], size_t n, uint16_t* const corr[3],
+                          void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* DistanceComparator: opening, rotation OR, candidate lists and merges.     */
+/* (iris-mpc-gpu/src/dot/distance_comparator.rs:28-894)                      */
+/* ------------------------------------------------------------------------ */
+typedef struct irs_distance_comparator irs_distance_comparator;
+
+/* DistanceComparator::init (distance_comparator.rs:58-190). */
+int irs_dc_init(irs_device_manager* dm, size_t max_queries, size_t max_db_length, size_t match_list_cap,
+                irs_distance_comparator** out);
+int irs_dc_destroy(irs_distance_comparator* dc);
+/* Clears bitmaps, counters and final results for a new batch. */
+int irs_dc_reset(irs_distance_comparator* dc, void* stream);
+
+/* The hot step of compare_query_against_db_and_self_prefiltering
+ * (iris-mpc-gpu/src/server/actor.rs:2405-2519): for the six engines' current
+ * results over entries [offset, offset+len), runs the threshold protocol,
+ * opens the bits (open, actor.rs:2928-2997), ORs every slot's valid rotation
+ * rows (openResults, dot/kernel.cu:54-116) into the match bitmap and appends
+ * (query, entry) pairs to the match list.  slot_valid[s]: bit mask of valid
+ * rows of slot s (NULL = rows 0..30); slot_query[s]: bitmap row of slot s
+ * (NULL = s).  `self_check` != 0 writes the batch-self bitmap instead. */
+int irs_dc_compare_threshold_open(irs_distance_comparator* dc, irs_circuits* c, irs_sharedb* const code_engines[3],
+                                  irs_sharedb* const mask_engines[3], size_t offset, size_t len, size_t n_slots,
+                                  const uint32_t* slot_valid, const uint32_t* slot_query, uint32_t threshold_a,
+                                  int self_check, void* stream);
+/* Match bitmap in the reference layout: bit (q * db_len + e) set if query q
+ * matches entry e (u64 words, ceil(n_queries * db_len / 64)). */
+int irs_dc_fetch_bitmap(irs_distance_comparator* dc, size_t n_queries, size_t db_len, uint64_t* host);
+/* Matches (query, entry) pairs appended since the last reset. */
+int irs_dc_fetch_matches(irs_distance_comparator* dc, uint32_t* pairs, size_t cap, size_t* n);
+/* get_partial_results (distance_comparator.rs:545-646, partialDbResults):
+ * sorted unique entry indices matched by any query; *n may exceed cap
+ * (overflow is reported as IRS_ERR_OVERFLOW after filling cap ids). */
+int irs_dc_get_partial_results(irs_distance_comparator* dc, size_t n_queries, size_t db_len, uint32_t* ids,
+                               size_t cap, size_t* n);
+/* join_db_matches(_with_bitmaps) (distance_comparator.rs:688-729): merges the
+ * DB bitmap of this comparator (left eye) with `right` (NULL: single eye) and
+ * an optional OR-policy bitmap (device, same layout as the internal bitmap);
+ * final results per query = smallest matched entry. */
+int irs_dc_join_db_matches(irs_distance_comparator* dc, irs_distance_comparator* right, const uint32_t* or_policy,
+                           size_t n_queries, size_t db_len, void* stream);
+/* join_batch_matches (distance_comparator.rs:731-746, mergeBatchResults). */
+int irs_dc_join_batch_matches(irs_distance_comparator* dc, irs_distance_comparator* right, size_t n_queries,
+                              void* stream);
+/* fetch_final_results / fetch_match_counters / fetch_all_match_ids
+ * (distance_comparator.rs:748-893): final[q] = smallest matched entry,
+ * 0xFFFFFFFE for an in-batch duplicate, 0xFFFFFFFF for no match. */
+int irs_dc_fetch_final_results(irs_distance_comparator* dc, size_t n_queries, uint32_t* final_results,
+                               uint32_t* match_counters, uint32_t* all_matches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IRISB200_H */

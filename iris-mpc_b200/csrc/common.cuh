@@ -1,0 +1,110 @@
+// Shared device helpers for the iris B200 kernels: ChaCha12 keystream blocks,
+// the position-addressable keystream layout, error reporting and bounded
+// waits.  Everything here is __host__ __device__ where it can be, so the
+// host-side unit harness exercises the same code the kernels run.
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#define IRS_HD __host__ __device__ __forceinline__
+
+namespace irs {
+
+constexpr int kIrisCodeLength = 12800;
+constexpr int kMaskCodeLength = 6400;
+constexpr int kRotations = 31;
+constexpr int kRowLen = 800;        // coefficients per iris row (200 columns x 4)
+constexpr int kSlotRows = 32;       // query rows reserved per query iris (31 rotations + 1 pad)
+
+// Keystream domains: nonce = (domain << 32) | device index.
+constexpr uint32_t kDomCodeDot = 1;
+constexpr uint32_t kDomMaskDot = 2;
+constexpr uint32_t kDomCircuit = 3;
+// Circuit keystream: 8 blocks (128 words) per 32-element word and stream.
+constexpr int kCircuitBlocksPerWord = 8;
+
+// Threshold circuit variants: the full compare_threshold_masked_many, or the
+// msb of -code*2^16 - 1 alone (lifted mask and corrections at zero).
+enum : int { kStageFull = 0, kStageMsbOnly = 1 };
+
+// Error codes written to the device error word (first error wins).
+enum : int {
+  kErrNone = 0,
+  kErrTimeoutFull = 1,      // MMA waited too long for a TMA stage
+  kErrTimeoutEmpty = 2,     // producer waited too long for a free stage
+  kErrTimeoutAccFull = 3,   // epilogue waited too long for the accumulator
+  kErrTimeoutAccEmpty = 4,  // MMA waited too long for the epilogue
+  kErrTimeoutDrain = 5,     // exit-time wait on in-flight copies gave up
+  kErrBadShape = 6,
+  kErrOverflow = 7,         // a result list exceeded its capacity (counted, not fatal)
+};
+
+IRS_HD uint64_t nonce_of(uint32_t domain, uint32_t dev) { return ((uint64_t)domain << 32) | dev; }
+IRS_HD uint64_t counter_of(uint64_t batch, uint64_t blk) { return (batch << 40) | blk; }
+
+struct ChaChaKey {
+  uint32_t k[8];
+};
+
+IRS_HD uint32_t rotl32(uint32_t v, int n) {
+#ifdef __CUDA_ARCH__
+  return __funnelshift_l(v, v, n);
+#else
+  return (v << n) | (v >> (32 - n));
+#endif
+}
+
+#define IRS_QR(a, b, c, d)        \
+  a += b; d ^= a; d = rotl32(d, 16); \
+  c += d; b ^= c; b = rotl32(b, 12); \
+  a += b; d ^= a; d = rotl32(d, 8);  \
+  c += d; b ^= c; b = rotl32(b, 7);
+
+// One keystream block: state = "expand 32-byte k" | key | counter | nonce,
+// ROUNDS/2 double rounds, feed-forward add.  Same construction as the
+// reference's chacha12 kernel (iris-mpc-gpu/src/rng/chacha.cu:74-138), with
+// the whole state in registers.
+template <int ROUNDS = 12>
+IRS_HD void chacha_block(const ChaChaKey& key, uint64_t counter, uint64_t nonce, uint32_t out[16]) {
+  const uint32_t c0 = 0x61707865u, c1 = 0x3320646eu, c2 = 0x79622d32u, c3 = 0x6b206574u;
+  uint32_t x0 = c0, x1 = c1, x2 = c2, x3 = c3;
+  uint32_t x4 = key.k[0], x5 = key.k[1], x6 = key.k[2], x7 = key.k[3];
+  uint32_t x8 = key.k[4], x9 = key.k[5], x10 = key.k[6], x11 = key.k[7];
+  uint32_t x12 = (uint32_t)counter, x13 = (uint32_t)(counter >> 32);
+  uint32_t x14 = (uint32_t)nonce, x15 = (uint32_t)(nonce >> 32);
+#pragma unroll
+  for (int i = 0; i < ROUNDS / 2; i++) {
+    IRS_QR(x0, x4, x8, x12) IRS_QR(x1, x5, x9, x13) IRS_QR(x2, x6, x10, x14) IRS_QR(x3, x7, x11, x15)
+    IRS_QR(x0, x5, x10, x15) IRS_QR(x1, x6, x11, x12) IRS_QR(x2, x7, x8, x13) IRS_QR(x3, x4, x9, x14)
+  }
+  out[0] = x0 + c0; out[1] = x1 + c1; out[2] = x2 + c2; out[3] = x3 + c3;
+  out[4] = x4 + key.k[0]; out[5] = x5 + key.k[1]; out[6] = x6 + key.k[2]; out[7] = x7 + key.k[3];
+  out[8] = x8 + key.k[4]; out[9] = x9 + key.k[5]; out[10] = x10 + key.k[6]; out[11] = x11 + key.k[7];
+  out[12] = x12 + (uint32_t)counter; out[13] = x13 + (uint32_t)(counter >> 32);
+  out[14] = x14 + (uint32_t)nonce; out[15] = x15 + (uint32_t)(nonce >> 32);
+}
+#undef IRS_QR
+
+// Packed 16-bit lane arithmetic (two u16 per u32, no carry across lanes).
+IRS_HD uint32_t add2(uint32_t a, uint32_t b) {
+  return ((a & 0x7fff7fffu) + (b & 0x7fff7fffu)) ^ ((a ^ b) & 0x80008000u);
+}
+IRS_HD uint32_t sub2(uint32_t a, uint32_t b) {
+  return ((a | 0x80008000u) - (b & 0x7fff7fffu)) ^ ((a ^ ~b) & 0x80008000u);
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void set_error(int* err, int code) {
+  if (err) atomicCAS(err, 0, code);
+}
+__device__ __forceinline__ bool has_error(const int* err) {
+  return err && *(const volatile int*)err != 0;
+}
+#endif
+
+}  // namespace irs

@@ -1,0 +1,417 @@
+// Exact mod-2^16 dot products of u16 share matrices on tcgen05 INT8 tensor cores.
+//
+// Replaces the reference's three cublasGemmEx int8 limb GEMMs plus the
+// matmul_correct_and_reduce kernel (iris-mpc-gpu/src/dot/share_db.rs:62-112,
+// 800-905; iris-mpc-gpu/src/dot/kernel.cu:16-28).  Each u16 is split into two
+// unsigned bytes (lo, hi); since
+//     d*q mod 2^16 = dlo*qlo + 2^8 * (dlo*qhi + dhi*qlo)   (mod 2^16)
+// one pass over K issues three u8 x u8 -> s32 MMAs per K step into two TMEM
+// accumulators: acc0 += Dlo.Qlo and acc1 += Dlo.Qhi + Dhi.Qlo.  The epilogue
+// forms (acc0 + (acc1 << 8)) mod 2^16, multiplies by the engine multiplier
+// (2 for trimmed masks), adds the zero-share mask ks_own - ks_prev computed in
+// registers with ChaCha12, and stores u16 dot shares.  Unsigned limbs need no
+// sum correction (the reference's signed limbs do).
+//
+// Layouts: DB limb planes [entries][K] u8, query limb planes [rows][K] u8
+// (both K-major, K a multiple of 128), output [entries][n_pad] u16 with the
+// query row fastest.  Keystream u16 of element (entry m, row n) sits at index
+// m * n_pad + n of the engine's stream (32 u16 per ChaCha block).
+//
+// Kernel structure (one CTA per SM, persistent over tiles of 128 entries x BN
+// rows): warp 0 issues TMA loads (128B swizzle) into a STAGES-deep ring,
+// warp 1 allocates TMEM and issues the MMAs from one thread, warps 2..9 drain
+// the accumulators (tcgen05.ld), release TMEM to the next tile and then run
+// the ChaCha mask and the stores while the next tile's MMAs proceed.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include "common.cuh"
+#include "gemm_limb.h"
+
+namespace irs {
+
+namespace {
+
+constexpr int kBM = 128;   // DB entries per tile (MMA M)
+constexpr int kBK = 128;   // K bytes per pipeline stage (one 128-byte swizzle row)
+constexpr int kThreads = 320;
+constexpr uint64_t kWaitTimeoutNs = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after kWaitTimeoutNs or when another thread has
+// reported an error, recording `code` in the error word.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t it = 1;; it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0) {
+      if (has_error(err)) return false;
+      if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+        set_error(err, code);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), version 1, layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t smem_desc(const void* p) {
+  const uint64_t addr = smem_u32(p);
+  return ((addr & 0x3FFFFull) >> 4) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// Instruction descriptor: u8 x u8 -> s32, K-major A and B, M = 128, N = BN.
+__host__ __device__ constexpr uint32_t idesc_u8(int bn) {
+  return (2u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_u8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+template <int BN>
+struct Cfg {
+  static constexpr int kStageBytes = 2 * kBM * kBK + 2 * BN * kBK;
+  static constexpr int kStages = (196608 / kStageBytes) > 6 ? 6 : (196608 / kStageBytes);
+  static constexpr int kTmemCols = 2 * BN;  // acc0 | acc1
+  static constexpr int kColsPerThread = BN / 2;  // two epilogue warps per TMEM lane quadrant
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+};
+
+struct Tile {
+  int prob, m_tile, n_tile;
+};
+
+__device__ __forceinline__ bool tile_of(const GemmParams& P, int t, Tile& out) {
+  for (int i = 0; i < P.n_prob; i++) {
+    const int nt = (int)(P.prob[i].tiles_m * P.prob[i].tiles_n);
+    if (t < nt) {
+      out.prob = i;
+      out.m_tile = t / (int)P.prob[i].tiles_n;
+      out.n_tile = t % (int)P.prob[i].tiles_n;
+      return true;
+    }
+    t -= nt;
+  }
+  return false;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_constant__ GemmParams P) {
+  using C = Cfg<BN>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* a_lo = smem;
+  uint8_t* a_hi = a_lo + C::kStages * kBM * kBK;
+  uint8_t* b_lo = a_hi + C::kStages * kBM * kBK;
+  uint8_t* b_hi = b_lo + C::kStages * BN * kBK;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(b_hi + C::kStages * BN * kBK);
+  uint64_t* full_bar = bars;
+  uint64_t* empty_bar = bars + C::kStages;
+  uint64_t* acc_full = bars + 2 * C::kStages;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* done_bar = acc_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 3);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int* err = P.err;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::kStages; s++) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 8);  // one arrive per epilogue warp
+    mbar_init(done_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)C::kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int issued_phase[8];
+      bool issued[8];
+      for (int s = 0; s < C::kStages; s++) issued[s] = false;
+      bool ok = true;
+      for (int t = blockIdx.x; ok && t < P.total_tiles; t += gridDim.x) {
+        Tile tl;
+        if (!tile_of(P, t, tl)) break;
+        const GemmProblem& pr = P.prob[tl.prob];
+        const int ya = (int)pr.m0 + tl.m_tile * kBM;
+        const int yb = tl.n_tile * BN;
+        for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1u, err, kErrTimeoutEmpty)) { ok = false; break; }
+          mbar_expect_tx(&full_bar[stage], (uint32_t)C::kStageBytes);
+          const int x = (int)ki * kBK;
+          tma_load_2d(a_lo + stage * kBM * kBK, &pr.tm_a_lo, &full_bar[stage], x, ya);
+          tma_load_2d(a_hi + stage * kBM * kBK, &pr.tm_a_hi, &full_bar[stage], x, ya);
+          tma_load_2d(b_lo + stage * BN * kBK, &pr.tm_b_lo, &full_bar[stage], x, yb);
+          tma_load_2d(b_hi + stage * BN * kBK, &pr.tm_b_hi, &full_bar[stage], x, yb);
+          issued[stage] = true;
+          issued_phase[stage] = (int)phase;
+          if (++stage == C::kStages) { stage = 0; phase ^= 1u; }
+        }
+      }
+      // Exit: make sure no copy into this CTA's shared memory is still in flight.
+      for (int s = 0; s < C::kStages; s++)
+        if (issued[s]) mbar_wait(&full_bar[s], (uint32_t)issued_phase[s], err, kErrTimeoutDrain);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t acc_phase = 0;
+      bool ok = true;
+      constexpr uint32_t idesc = idesc_u8(BN);
+      for (int t = blockIdx.x; ok && t < P.total_tiles; t += gridDim.x) {
+        Tile tl;
+        if (!tile_of(P, t, tl)) break;
+        const GemmProblem& pr = P.prob[tl.prob];
+        if (!mbar_wait(acc_empty, acc_phase ^ 1u, err, kErrTimeoutAccEmpty)) { ok = false; break; }
+        acc_phase ^= 1u;
+        tc_fence_after();
+        for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
+          if (!mbar_wait(&full_bar[stage], phase, err, kErrTimeoutFull)) { ok = false; break; }
+          tc_fence_after();
+          const uint64_t dal = smem_desc(a_lo + stage * kBM * kBK);
+          const uint64_t dah = smem_desc(a_hi + stage * kBM * kBK);
+          const uint64_t dbl = smem_desc(b_lo + stage * BN * kBK);
+          const uint64_t dbh = smem_desc(b_hi + stage * BN * kBK);
+#pragma unroll
+          for (int kk = 0; kk < kBK / 32; kk++) {
+            const uint32_t acc = (ki > 0 || kk > 0) ? 1u : 0u;
+            const uint64_t o = (uint64_t)(2 * kk);  // 32 bytes along K, in 16-byte units
+            mma_u8(tmem, dal + o, dbl + o, idesc, acc);
+            mma_u8(tmem + BN, dal + o, dbh + o, idesc, acc);
+            mma_u8(tmem + BN, dah + o, dbl + o, idesc, 1u);
+          }
+          mma_commit(&empty_bar[stage]);
+          if (++stage == C::kStages) { stage = 0; phase ^= 1u; }
+        }
+        if (ok) mma_commit(acc_full);
+      }
+      // Exit: wait until every MMA issued by this thread has completed.
+      mma_commit(done_bar);
+      mbar_wait(done_bar, 0, err, kErrTimeoutDrain);
+    }
+  } else {
+    // ---------------- Epilogue (warps 2..9) ----------------
+    const int quad = warp & 3;                 // TMEM lanes 32*quad .. 32*quad+31
+    const int half = (warp - 2) >> 2;          // column half of the tile
+    const int row = quad * 32 + lane;          // entry within the tile
+    constexpr int kCols = C::kColsPerThread;
+    uint32_t acc_phase = 0;
+    for (int t = blockIdx.x; t < P.total_tiles; t += gridDim.x) {
+      Tile tl;
+      if (!tile_of(P, t, tl)) break;
+      const GemmProblem& pr = P.prob[tl.prob];
+      if (!mbar_wait(acc_full, acc_phase, err, kErrTimeoutAccFull)) break;
+      acc_phase ^= 1u;
+      tc_fence_after();
+      uint32_t packed[kCols / 2];
+      const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * kCols);
+#pragma unroll
+      for (int c = 0; c < kCols / 32; c++) {
+        uint32_t r0[32], r1[32];
+        tmem_ld32(tbase + (uint32_t)(c * 32), r0);
+        tmem_ld32(tbase + (uint32_t)(BN + c * 32), r1);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const uint32_t lo = (r0[2 * j] + (r1[2 * j] << 8)) & 0xFFFFu;
+          const uint32_t hi = (r0[2 * j + 1] + (r1[2 * j + 1] << 8)) << 16;
+          packed[c * 16 + j] = lo | hi;
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty);
+
+      const uint32_t m_local = (uint32_t)(tl.m_tile * kBM + row);
+      if (m_local < pr.m_len) {
+        const uint64_t m_global = (uint64_t)pr.m0 + m_local;
+        uint16_t* out_row = pr.out + (size_t)m_local * pr.n_pad;
+#pragma unroll
+        for (int c = 0; c < kCols / 32; c++) {
+          const uint32_t n = (uint32_t)(tl.n_tile * BN + half * kCols + c * 32);
+          uint32_t v[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const uint32_t x = packed[c * 16 + j];
+            v[j] = (pr.mult == 1) ? x : (((x & 0xFFFFu) * pr.mult) & 0xFFFFu) | (((x >> 16) * pr.mult) << 16);
+          }
+          if (pr.mask_on) {
+            const uint64_t blk = (m_global * pr.n_pad + n) >> 5;
+            uint32_t ko[16], kp[16];
+            chacha_block<12>(pr.key_own, counter_of(pr.batch, blk), pr.nonce, ko);
+            chacha_block<12>(pr.key_prev, counter_of(pr.batch, blk), pr.nonce, kp);
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = sub2(add2(v[j], ko[j]), kp[j]);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(out_row + n);
+#pragma unroll
+          for (int q = 0; q < 4; q++) dst[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)C::kTmemCols));
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+int make_tmap_u8(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k, uint32_t box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return -1;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (k % kBK) || box_rows > 256) return -2;
+  cuuint64_t dims[2] = {k, rows};
+  cuuint64_t strides[1] = {k};
+  cuuint32_t box[2] = {(cuuint32_t)kBK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -3;
+}
+
+template <int BN>
+static cudaError_t launch_bn(const GemmParams& P, int n_sms, cudaStream_t stream) {
+  using C = Cfg<BN>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(limb_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         C::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  const int grid = P.total_tiles < n_sms ? P.total_tiles : n_sms;
+  if (grid <= 0) return cudaSuccess;
+  limb_gemm_kernel<BN><<<grid, kThreads, C::kSmemBytes, stream>>>(P);
+  return cudaGetLastError();
+}
+
+int gemm_block_n_for(uint32_t n_pad) {
+  if (n_pad % 256 == 0) return 256;
+  if (n_pad % 128 == 0) return 128;
+  if (n_pad % 64 == 0) return 64;
+  return 0;
+}
+
+cudaError_t launch_limb_gemm(GemmParams& P, int block_n, int n_sms, cudaStream_t stream) {
+  P.total_tiles = 0;
+  for (int i = 0; i < P.n_prob; i++) {
+    GemmProblem& pr = P.prob[i];
+    pr.tiles_m = (pr.m_len + kBM - 1) / kBM;
+    pr.tiles_n = pr.n_pad / (uint32_t)block_n;
+    P.total_tiles += (int)(pr.tiles_m * pr.tiles_n);
+  }
+  switch (block_n) {
+    case 256: return launch_bn<256>(P, n_sms, stream);
+    case 128: return launch_bn<128>(P, n_sms, stream);
+    case 64: return launch_bn<64>(P, n_sms, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace irs

@@ -1,0 +1,50 @@
+// Launch interface of the tcgen05 limb GEMM (internal to the library).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "common.cuh"
+
+namespace irs {
+
+// One dot-product problem: a party's DB limb planes against its query limb
+// planes, for the entries [m0, m0 + m_len).
+struct alignas(64) GemmProblem {
+  CUtensorMap tm_a_lo;  // DB low bytes   [rows][K]
+  CUtensorMap tm_a_hi;  // DB high bytes  [rows][K]
+  CUtensorMap tm_b_lo;  // query low bytes  [n_pad][K]
+  CUtensorMap tm_b_hi;  // query high bytes [n_pad][K]
+  uint16_t* out;        // [m_len][n_pad]
+  uint32_t m0;
+  uint32_t m_len;
+  uint32_t n_pad;
+  uint32_t k_iters;     // K / 128
+  uint32_t mult;        // 1 for codes, 2 for trimmed masks
+  uint32_t mask_on;     // add ks_own - ks_prev
+  ChaChaKey key_own;
+  ChaChaKey key_prev;
+  uint64_t nonce;
+  uint64_t batch;
+  uint32_t tiles_m;     // filled by launch_limb_gemm
+  uint32_t tiles_n;
+};
+
+constexpr int kMaxGemmProblems = 6;
+
+struct GemmParams {
+  GemmProblem prob[kMaxGemmProblems];
+  int n_prob;
+  int total_tiles;
+  int* err;
+};
+
+// Builds a 2-D u8 tensor map (inner dim K, outer dim rows) with 128x`box_rows`
+// boxes and 128-byte swizzle.  Returns 0 on success.
+int make_tmap_u8(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k, uint32_t box_rows);
+
+// Tile width along the query rows that divides n_pad (256, 128 or 64; 0 if none).
+int gemm_block_n_for(uint32_t n_pad);
+
+cudaError_t launch_limb_gemm(GemmParams& P, int block_n, int n_sms, cudaStream_t stream);
+
+}  // namespace irs

@@ -1,0 +1,144 @@
+// Fused 3-party threshold comparison, open and rotation OR.
+//
+// One thread evaluates the whole Phase-2 protocol for one 32-element word of
+// all three co-resident parties (circuit.cuh): the lift of the mask dot
+// shares from Z_2^16 to Z_2^32, the bit injection of the two lift carries,
+// mask*A - code*2^16 - 1, the 32-bit MSB adder, and the opening of the result.
+// The per-gate "send to next party" of the reference (NCCL send/recv around
+// every AND round, iris-mpc-gpu/src/threshold_ring/protocol.rs:894-1032) is the
+// component store inside the thread, so the ~52 dependent rounds and ~7
+// launches per round collapse into straight-line code, and HBM sees each input
+// share exactly once.
+//
+// Modes:
+//   flat   -- elements e = 0..n-1, word w = e/32 (Circuits API: results are
+//             the per-party shares of the msb bit plus the opened bits);
+//   bitmap -- dot shares laid out [entry][n_pad], each query iris owning a
+//             32-row slot; a warp covers 32 consecutive entries of one slot,
+//             the opened word OR-ed over the slot's valid rows is the match bit
+//             (the rotation OR of openResults, dot/kernel.cu:54-116), written
+//             with one ballot per warp, and matches are appended to a list.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "circuit.cuh"
+#include "threshold.h"
+
+namespace irs {
+
+namespace {
+
+constexpr int kThreshThreads = 128;
+
+__device__ __forceinline__ void init_rand(WordRand& wr, const ThresholdParams& P, uint64_t word_id) {
+#pragma unroll
+  for (int s = 0; s < 3; s++) wr.key[s] = P.key[s];
+  wr.nonce = P.nonce;
+  wr.base = counter_of(P.batch, word_id * (uint64_t)kCircuitBlocksPerWord);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(kThreshThreads) threshold_flat_kernel(const ThresholdParams P) {
+  const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.n_words) return;
+  WordRand wr;
+  init_rand(wr, P, P.word_base + w);
+  const uint16_t* code[3] = {P.code[0] + 32 * w, P.code[1] + 32 * w, P.code[2] + 32 * w};
+  const uint16_t* mask[3] = {P.mask[0] + 32 * w, P.mask[1] + 32 * w, P.mask[2] + 32 * w};
+  Comp msb;
+  const uint32_t r = threshold_word<STAGE>(code, mask, P.threshold_a, wr, msb);
+  if (P.revealed) P.revealed[w] = r;
+  if (P.res_comp) {
+    P.res_comp[w] = msb.c0;
+    P.res_comp[P.n_words + w] = msb.c1;
+    P.res_comp[2 * P.n_words + w] = msb.c2;
+  }
+}
+
+__global__ void __launch_bounds__(kThreshThreads) threshold_bitmap_kernel(const ThresholdParams P) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t n_groups = (P.n_entries + 31) / 32;
+  const uint64_t total = (uint64_t)n_groups * P.n_slots;
+  if (gwarp >= total) return;  // warp-uniform
+  const uint32_t slot = (uint32_t)(gwarp % P.n_slots);
+  const uint32_t group = (uint32_t)(gwarp / P.n_slots);
+  const uint32_t m_local = group * 32 + lane;
+  const bool valid = m_local < P.n_entries;
+  const uint32_t m_read = valid ? m_local : (P.n_entries - 1);
+  const uint64_t m_global = (uint64_t)P.m0 + m_local;
+
+  WordRand wr;
+  init_rand(wr, P, ((uint64_t)P.m0 + m_read) * (uint64_t)(P.n_pad / 32) + slot);
+  const size_t off = (size_t)m_read * P.n_pad + (size_t)slot * 32;
+  const uint16_t* code[3] = {P.code[0] + off, P.code[1] + off, P.code[2] + off};
+  const uint16_t* mask[3] = {P.mask[0] + off, P.mask[1] + off, P.mask[2] + off};
+  Comp msb;
+  const uint32_t opened = threshold_word<kStageFull>(code, mask, P.threshold_a, wr, msb);
+  const uint32_t row_mask = P.slot_valid ? P.slot_valid[slot] : 0x7FFFFFFFu;
+  const bool match = valid && (opened & row_mask) != 0;
+  const uint32_t bits = __ballot_sync(0xFFFFFFFFu, match);
+  if (P.bitmap && lane == 0) {
+    const uint32_t query = P.slot_query ? P.slot_query[slot] : slot;
+    P.bitmap[(size_t)query * (P.bitmap_stride / 32) + (uint32_t)((P.m0 + group * 32) / 32)] = bits;
+  }
+  if (P.match_list && bits) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(P.match_count, (uint32_t)__popc(bits));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (match) {
+      const uint32_t rank = (uint32_t)__popc(bits & ((1u << lane) - 1u));
+      const uint32_t pos = base + rank;
+      if (pos < P.match_cap) {
+        const uint32_t query = P.slot_query ? P.slot_query[slot] : slot;
+        P.match_list[2 * pos] = query;
+        P.match_list[2 * pos + 1] = (uint32_t)m_global;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreshThreads) lift_flat_kernel(const ThresholdParams P, uint16_t* corr) {
+  const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.n_words) return;
+  WordRand wr;
+  init_rand(wr, P, P.word_base + w);
+  const uint16_t* mask[3] = {P.mask[0] + 32 * w, P.mask[1] + 32 * w, P.mask[2] + 32 * w};
+  uint16_t c1[3][32], c2[3][32];
+  lift_word(mask, wr, c1, c2);
+  const uint64_t n = P.n_words * 32;
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+    uint16_t* o1 = corr + (size_t)(2 * p) * n + 32 * w;
+    uint16_t* o2 = corr + (size_t)(2 * p + 1) * n + 32 * w;
+#pragma unroll
+    for (int j = 0; j < 32; j++) { o1[j] = c1[p][j]; o2[j] = c2[p][j]; }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_threshold_flat(const ThresholdParams& P, int stage, cudaStream_t stream) {
+  if (P.n_words == 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((P.n_words + kThreshThreads - 1) / kThreshThreads);
+  if (stage == kStageFull) threshold_flat_kernel<kStageFull><<<grid, kThreshThreads, 0, stream>>>(P);
+  else threshold_flat_kernel<kStageMsbOnly><<<grid, kThreshThreads, 0, stream>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_threshold_bitmap(const ThresholdParams& P, cudaStream_t stream) {
+  if (P.n_entries == 0 || P.n_slots == 0) return cudaSuccess;
+  const uint64_t warps = (uint64_t)((P.n_entries + 31) / 32) * P.n_slots;
+  const uint64_t threads = warps * 32;
+  const unsigned grid = (unsigned)((threads + kThreshThreads - 1) / kThreshThreads);
+  threshold_bitmap_kernel<<<grid, kThreshThreads, 0, stream>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lift_flat(const ThresholdParams& P, uint16_t* corr, cudaStream_t stream) {
+  if (P.n_words == 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((P.n_words + kThreshThreads - 1) / kThreshThreads);
+  lift_flat_kernel<<<grid, kThreshThreads, 0, stream>>>(P, corr);
+  return cudaGetLastError();
+}
+
+}  // namespace irs

@@ -1,0 +1,403 @@
+"""Host-side mirror of the iris-mpc GPU engines over the irisb200 C ABI.
+
+The classes follow the reference's Rust call surface for the uniqueness hot
+path -- ``ShareDB`` (iris-mpc-gpu/src/dot/share_db.rs), ``Circuits``
+(iris-mpc-gpu/src/threshold_ring/protocol.rs) and ``DistanceComparator``
+(iris-mpc-gpu/src/dot/distance_comparator.rs) -- with the three parties
+co-resident on one B200.  Every call goes through ``libirisb200.so``; there is
+no CPU fallback: importing this package on a machine without the built library
+raises, and constructing a device manager without a B200 raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libirisb200.so")
+
+IRIS_CODE_LENGTH = 12800
+MASK_CODE_LENGTH = 6400
+ROTATIONS = 31
+SLOT_ROWS = 32
+MAX_MATCHES_LEN = 256
+THRESHOLD_A = 20316          # ratio 0.345 (iris-mpc-gpu/src/dot/mod.rs:12)
+THRESHOLD_ANON_STATS_A = 16384  # ratio 0.375 (iris-mpc-gpu/src/dot/mod.rs:14)
+
+IRS_OK = 0
+IRS_ERR_OVERFLOW = -6
+
+
+class IrisError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"irisb200 error {code}: {msg}")
+        self.code = code
+
+
+class QuerySlot(C.Structure):
+    _fields_ = [("src", C.c_uint32), ("rot_lo", C.c_uint32), ("n_rot", C.c_uint32), ("query", C.c_uint32)]
+
+
+_vp = C.c_void_p
+_sz = C.c_size_t
+_u32 = C.c_uint32
+_u64 = C.c_uint64
+_i = C.c_int
+
+# name -> argtypes (all return int status unless listed in _RESTYPES)
+_SIGS = {
+    "irs_last_error": [],
+    "irs_version": [],
+    "irs_device_manager_init": [_i, C.POINTER(_vp)],
+    "irs_device_manager_destroy": [_vp],
+    "irs_device_manager_stream": [_vp, _i, C.POINTER(_vp)],
+    "irs_device_manager_synchronize": [_vp],
+    "irs_device_manager_error": [_vp, C.POINTER(_i)],
+    "irs_device_manager_clear_error": [_vp],
+    "irs_device_manager_sm_count": [_vp, C.POINTER(_i)],
+    "irs_device_alloc": [_vp, _sz, C.POINTER(_vp)],
+    "irs_device_free": [_vp, _vp],
+    "irs_copy_h2d": [_vp, _vp, _sz, _vp],
+    "irs_copy_d2h": [_vp, _vp, _sz, _vp],
+    "irs_stream_synchronize": [_vp],
+    "irs_sharedb_init": [_vp, _i, _sz, _sz, _sz, _vp, _vp, _i, C.POINTER(_vp)],
+    "irs_sharedb_destroy": [_vp],
+    "irs_sharedb_alloc_db": [_vp, _sz],
+    "irs_sharedb_load_records": [_vp, _sz, _sz, _vp],
+    "irs_sharedb_load_records_i8": [_vp, _sz, _sz, _vp, _vp],
+    "irs_sharedb_fetch_records": [_vp, _sz, _sz, _vp],
+    "irs_sharedb_set_db_len": [_vp, _sz],
+    "irs_sharedb_db_len": [_vp, C.POINTER(_sz)],
+    "irs_sharedb_synth_db": [_vp, _vp, _u64, _sz, _sz],
+    "irs_sharedb_query_upload": [_vp, _vp, _sz],
+    "irs_sharedb_query_upload_slots": [_vp, _vp, _sz, _vp, _sz],
+    "irs_sharedb_set_batch": [_vp, _u64],
+    "irs_sharedb_dot": [_vp, _sz, _sz, C.c_uint16, _vp],
+    "irs_sharedb_dot_many": [_vp, _vp, _i, _sz, _sz, _vp],
+    "irs_sharedb_fetch_results": [_vp, _vp, _sz],
+    "irs_sharedb_result_view": [_vp, C.POINTER(_vp), C.POINTER(_sz)],
+    "irs_circuits_new": [_vp, _vp, C.POINTER(_vp)],
+    "irs_circuits_destroy": [_vp],
+    "irs_circuits_set_batch": [_vp, _u64],
+    "irs_circuits_compare_threshold_masked_many": [_vp, _vp, _vp, _sz, _u32, _vp, _vp, _vp, _vp],
+    "irs_circuits_extract_msb_of_code": [_vp, _vp, _sz, _vp, _vp, _vp, _vp],
+    "irs_circuits_lift_mpc": [_vp, _vp, _sz, _vp, _vp],
+    "irs_dc_init": [_vp, _sz, _sz, _sz, C.POINTER(_vp)],
+    "irs_dc_destroy": [_vp],
+    "irs_dc_reset": [_vp, _vp],
+    "irs_dc_compare_threshold_open": [_vp, _vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp, _u32, _i, _vp],
+    "irs_dc_fetch_bitmap": [_vp, _sz, _sz, _vp],
+    "irs_dc_fetch_matches": [_vp, _vp, _sz, C.POINTER(_sz)],
+    "irs_dc_get_partial_results": [_vp, _sz, _sz, _vp, _sz, C.POINTER(_sz)],
+    "irs_dc_join_db_matches": [_vp, _vp, _vp, _sz, _sz, _vp],
+    "irs_dc_join_batch_matches": [_vp, _vp, _sz, _vp],
+    "irs_dc_fetch_final_results": [_vp, _sz, _vp, _vp, _vp],
+}
+_RESTYPES = {"irs_last_error": C.c_char_p, "irs_version": C.c_char_p}
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """Loads libirisb200.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run iris-mpc_b200/build.py (the CUDA library is required)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _RESTYPES.get(name, C.c_int)
+        _LIB = L
+    return _LIB
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS.keys())
+
+
+def _check(rc: int, allow=()) -> int:
+    if rc != IRS_OK and rc not in allow:
+        raise IrisError(rc, lib().irs_last_error().decode(errors="replace"))
+    return rc
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _seed(s) -> np.ndarray:
+    return np.ascontiguousarray(np.array(s, dtype=np.uint32).reshape(8))
+
+
+class DeviceBuffer:
+    """A plain device allocation (for callers staging their own shares)."""
+
+    def __init__(self, dm: "DeviceManager", nbytes: int):
+        self.dm = dm
+        self.nbytes = nbytes
+        p = _vp()
+        _check(lib().irs_device_alloc(dm.h, nbytes, C.byref(p)))
+        self.ptr = p.value
+
+    @classmethod
+    def from_array(cls, dm: "DeviceManager", a: np.ndarray) -> "DeviceBuffer":
+        a = np.ascontiguousarray(a)
+        b = cls(dm, a.nbytes)
+        b.upload(a)
+        return b
+
+    def upload(self, a: np.ndarray, stream=None) -> None:
+        a = np.ascontiguousarray(a)
+        assert a.nbytes <= self.nbytes
+        _check(lib().irs_copy_h2d(self.ptr, _ptr(a), a.nbytes, stream))
+        _check(lib().irs_stream_synchronize(stream))
+
+    def download(self, dtype, count: int, stream=None) -> np.ndarray:
+        out = np.zeros(count, dtype)
+        _check(lib().irs_copy_d2h(_ptr(out), self.ptr, out.nbytes, stream))
+        _check(lib().irs_stream_synchronize(stream))
+        return out
+
+    def free(self) -> None:
+        if self.ptr:
+            lib().irs_device_free(self.dm.h, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class DeviceManager:
+    """DeviceManager (iris-mpc-gpu/src/helpers/device_manager.rs) for one GPU
+    hosting the three parties, each with its own stream and memory pool."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        _check(lib().irs_device_manager_init(device, C.byref(h)))
+        self.h = h.value
+        self.device = device
+
+    def stream(self, party: int):
+        s = _vp()
+        _check(lib().irs_device_manager_stream(self.h, party, C.byref(s)))
+        return s.value
+
+    def synchronize(self) -> None:
+        _check(lib().irs_device_manager_synchronize(self.h))
+
+    def error_code(self) -> int:
+        c = C.c_int()
+        _check(lib().irs_device_manager_error(self.h, C.byref(c)))
+        return c.value
+
+    def sm_count(self) -> int:
+        c = C.c_int()
+        _check(lib().irs_device_manager_sm_count(self.h, C.byref(c)))
+        return c.value
+
+    def close(self) -> None:
+        if self.h:
+            lib().irs_device_manager_destroy(self.h)
+            self.h = None
+
+
+class ShareDB:
+    """ShareDB (iris-mpc-gpu/src/dot/share_db.rs:448-1070) of one party."""
+
+    def __init__(self, peer_id: int, dm: DeviceManager, max_db_length: int, query_length: int, code_length: int,
+                 chacha_seeds, is_remote: bool = True):
+        h = _vp()
+        s0, s1 = _seed(chacha_seeds[0]), _seed(chacha_seeds[1])
+        _check(lib().irs_sharedb_init(dm.h, peer_id, max_db_length, query_length, code_length, _ptr(s0), _ptr(s1),
+                                      int(is_remote), C.byref(h)))
+        self.h = h.value
+        self.dm = dm
+        self.peer_id = peer_id
+        self.query_length = query_length
+        self.code_length = code_length
+
+    def alloc_db(self, max_db_length: int) -> None:
+        _check(lib().irs_sharedb_alloc_db(self.h, max_db_length))
+
+    def load_records(self, first: int, records: np.ndarray) -> None:
+        r = np.ascontiguousarray(records, np.uint16).reshape(-1, self.code_length)
+        _check(lib().irs_sharedb_load_records(self.h, first, r.shape[0], _ptr(r)))
+
+    def load_records_i8(self, first: int, limb0: np.ndarray, limb1: np.ndarray) -> None:
+        a = np.ascontiguousarray(limb0).view(np.uint8).reshape(-1, self.code_length)
+        b = np.ascontiguousarray(limb1).view(np.uint8).reshape(-1, self.code_length)
+        _check(lib().irs_sharedb_load_records_i8(self.h, first, a.shape[0], _ptr(a), _ptr(b)))
+
+    def fetch_records(self, first: int, n: int) -> np.ndarray:
+        out = np.zeros((n, self.code_length), np.uint16)
+        _check(lib().irs_sharedb_fetch_records(self.h, first, n, _ptr(out)))
+        return out
+
+    def set_db_len(self, n: int) -> None:
+        _check(lib().irs_sharedb_set_db_len(self.h, n))
+
+    def db_len(self) -> int:
+        n = _sz()
+        _check(lib().irs_sharedb_db_len(self.h, C.byref(n)))
+        return n.value
+
+    def query_upload(self, rows: np.ndarray) -> None:
+        r = np.ascontiguousarray(rows, np.uint16).reshape(-1, self.code_length)
+        _check(lib().irs_sharedb_query_upload(self.h, _ptr(r), r.shape[0]))
+
+    def query_upload_slots(self, base: np.ndarray, slots) -> None:
+        b = np.ascontiguousarray(base, np.uint16).reshape(-1, self.code_length)
+        arr = (QuerySlot * len(slots))(*[QuerySlot(*s) for s in slots])
+        _check(lib().irs_sharedb_query_upload_slots(self.h, _ptr(b), b.shape[0], C.cast(arr, _vp), len(slots)))
+
+    def set_batch(self, batch_id: int) -> None:
+        _check(lib().irs_sharedb_set_batch(self.h, batch_id))
+
+    def dot(self, offset: int, length: int, multiplier: int = 1, stream=None) -> None:
+        """dot + dot_reduce_and_multiply (share_db.rs:800-905), fused."""
+        _check(lib().irs_sharedb_dot(self.h, offset, length, multiplier, stream))
+
+    def fetch_results(self, length: int) -> np.ndarray:
+        out = np.zeros((self.query_length, length), np.uint16)
+        _check(lib().irs_sharedb_fetch_results(self.h, _ptr(out), length))
+        return out
+
+    def result_view(self):
+        p = _vp()
+        s = _sz()
+        _check(lib().irs_sharedb_result_view(self.h, C.byref(p), C.byref(s)))
+        return p.value, s.value
+
+    def close(self) -> None:
+        if self.h:
+            lib().irs_sharedb_destroy(self.h)
+            self.h = None
+
+
+def dot_many(engines, multipliers, offset: int, length: int, stream=None) -> None:
+    """One tcgen05 launch for several engines (e.g. 3 parties x code/mask)."""
+    hs = (_vp * len(engines))(*[e.h for e in engines])
+    ms = (C.c_uint16 * len(engines))(*multipliers)
+    _check(lib().irs_sharedb_dot_many(C.cast(hs, _vp), C.cast(ms, _vp), len(engines), offset, length, stream))
+
+
+def synth_db(code_engines, mask_engines, seed: int, first: int, n: int) -> None:
+    hc = (_vp * 3)(*[e.h for e in code_engines])
+    hm = (_vp * 3)(*[e.h for e in mask_engines])
+    _check(lib().irs_sharedb_synth_db(C.cast(hc, _vp), C.cast(hm, _vp), seed, first, n))
+
+
+def _ptr3(xs):
+    return C.cast((_vp * 3)(*[x if isinstance(x, int) else x.ptr for x in xs]), _vp)
+
+
+class Circuits:
+    """Circuits (iris-mpc-gpu/src/threshold_ring/protocol.rs:433-2611) of the
+    three co-resident parties.  seeds[p] = party p's (seed0, seed1)."""
+
+    def __init__(self, dm: DeviceManager, seeds):
+        arr = np.ascontiguousarray(np.array(seeds, dtype=np.uint32).reshape(3, 2, 8))
+        h = _vp()
+        _check(lib().irs_circuits_new(dm.h, _ptr(arr), C.byref(h)))
+        self.h = h.value
+        self.dm = dm
+
+    def set_batch(self, batch_id: int) -> None:
+        _check(lib().irs_circuits_set_batch(self.h, batch_id))
+
+    def compare_threshold_masked_many(self, code_a, mask_a, n: int, threshold_a: int, res_a=None, res_b=None,
+                                      opened=None, stream=None) -> None:
+        _check(lib().irs_circuits_compare_threshold_masked_many(
+            self.h, _ptr3(code_a), _ptr3(mask_a), n, threshold_a,
+            _ptr3(res_a) if res_a else None, _ptr3(res_b) if res_b else None,
+            opened.ptr if opened else None, stream))
+
+    def extract_msb_of_code(self, code_a, n: int, res_a=None, res_b=None, opened=None, stream=None) -> None:
+        _check(lib().irs_circuits_extract_msb_of_code(
+            self.h, _ptr3(code_a), n, _ptr3(res_a) if res_a else None, _ptr3(res_b) if res_b else None,
+            opened.ptr if opened else None, stream))
+
+    def lift_mpc(self, mask_a, n: int, corr, stream=None) -> None:
+        _check(lib().irs_circuits_lift_mpc(self.h, _ptr3(mask_a), n, _ptr3(corr), stream))
+
+    def close(self) -> None:
+        if self.h:
+            lib().irs_circuits_destroy(self.h)
+            self.h = None
+
+
+class DistanceComparator:
+    """DistanceComparator (iris-mpc-gpu/src/dot/distance_comparator.rs)."""
+
+    def __init__(self, dm: DeviceManager, max_queries: int, max_db_length: int, match_list_cap: int = 1 << 20):
+        h = _vp()
+        _check(lib().irs_dc_init(dm.h, max_queries, max_db_length, match_list_cap, C.byref(h)))
+        self.h = h.value
+        self.dm = dm
+        self.max_queries = max_queries
+
+    def reset(self, stream=None) -> None:
+        _check(lib().irs_dc_reset(self.h, stream))
+
+    def compare_threshold_open(self, circuits: Circuits, code_engines, mask_engines, offset: int, length: int,
+                               n_slots: int, threshold_a: int, slot_valid=None, slot_query=None,
+                               self_check: bool = False, stream=None) -> None:
+        hc = (_vp * 3)(*[e.h for e in code_engines])
+        hm = (_vp * 3)(*[e.h for e in mask_engines])
+        sv = np.ascontiguousarray(slot_valid, np.uint32) if slot_valid is not None else None
+        sq = np.ascontiguousarray(slot_query, np.uint32) if slot_query is not None else None
+        _check(lib().irs_dc_compare_threshold_open(
+            self.h, circuits.h, C.cast(hc, _vp), C.cast(hm, _vp), offset, length, n_slots,
+            _ptr(sv) if sv is not None else None, _ptr(sq) if sq is not None else None, threshold_a,
+            int(self_check), stream))
+
+    def fetch_bitmap(self, n_queries: int, db_len: int) -> np.ndarray:
+        """Reference layout: bit (q * db_len + e), u64 words."""
+        out = np.zeros((n_queries * db_len + 63) // 64, np.uint64)
+        _check(lib().irs_dc_fetch_bitmap(self.h, n_queries, db_len, _ptr(out)))
+        return out
+
+    def fetch_matches(self, cap: int = 1 << 20) -> np.ndarray:
+        out = np.zeros(2 * cap, np.uint32)
+        n = _sz()
+        _check(lib().irs_dc_fetch_matches(self.h, _ptr(out), cap, C.byref(n)))
+        return out[: 2 * min(n.value, cap)].reshape(-1, 2)
+
+    def get_partial_results(self, n_queries: int, db_len: int, cap: int = 1 << 20) -> np.ndarray:
+        out = np.zeros(cap, np.uint32)
+        n = _sz()
+        _check(lib().irs_dc_get_partial_results(self.h, n_queries, db_len, _ptr(out), cap, C.byref(n)))
+        return out[: min(n.value, cap)]
+
+    def join_db_matches(self, n_queries: int, db_len: int, right: "DistanceComparator" = None,
+                        or_policy=None, stream=None) -> None:
+        _check(lib().irs_dc_join_db_matches(self.h, right.h if right else None, or_policy, n_queries, db_len,
+                                            stream))
+
+    def join_batch_matches(self, n_queries: int, right: "DistanceComparator" = None, stream=None) -> None:
+        _check(lib().irs_dc_join_batch_matches(self.h, right.h if right else None, n_queries, stream))
+
+    def fetch_final_results(self, n_queries: int):
+        f = np.zeros(n_queries, np.uint32)
+        c = np.zeros(n_queries, np.uint32)
+        a = np.zeros((n_queries, MAX_MATCHES_LEN), np.uint32)
+        _check(lib().irs_dc_fetch_final_results(self.h, n_queries, _ptr(f), _ptr(c), _ptr(a)))
+        return f, c, a
+
+    def close(self) -> None:
+        if self.h:
+            lib().irs_dc_destroy(self.h)
+            self.h = None
+
+
+def bitmap_get(bitmap: np.ndarray, n_queries: int, db_len: int) -> np.ndarray:
+    """Unpacks a reference-layout bitmap into [n_queries][db_len] uint8."""
+    bits = np.unpackbits(bitmap.view(np.uint8), bitorder="little")[: n_queries * db_len]
+    return bits.reshape(n_queries, db_len)

@@ -1,0 +1,42 @@
+"""Shared pytest setup: import paths, the `gpu` marker, and helpers."""
+from __future__ import annotations
+
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "iris-mpc_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+REFERENCE = "/root/reference"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 and the built CUDA library")
+
+
+def reference_file(rel: str) -> str:
+    """Path of a reference data file; skips the test when the reference tree is absent."""
+    path = os.path.join(REFERENCE, rel)
+    if not os.path.exists(path):
+        pytest.skip(f"reference data {rel} not available on this machine")
+    return path
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import oracle as O
+    O.build()
+    return O
+
+
+@pytest.fixture(scope="session")
+def dm():
+    import irisb200
+    d = irisb200.DeviceManager(0)
+    yield d
+    d.close()
