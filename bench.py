@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Iris comparisons/sec of the 3-party uniqueness hot path on B200.
+
+Workload (the GPU plain drop-in configuration): 3 parties co-resident on one
+GPU, 64 queries x 31 rotations (1984 query rows in 64 slots of 32) against
+524,288 share-DB entries per party, threshold ratio 0.375 (A = 16384).  One
+step = one batch: the six limb GEMMs (3 parties x code/mask) in one tcgen05
+launch, then the fused threshold + open + rotation OR into the match bitmap.
+One comparison = one (query iris, DB entry) pair over all 31 rotations,
+computed jointly by the three parties.
+
+  value -- comparisons/s with the queries already expanded in HBM;
+  e2e   -- the same through the public API with host I/O inside every step:
+           H2D of the six engines' base query shares from pinned memory,
+           device-side rotation expansion, GEMMs, threshold, result merge and
+           D2H of the per-query results.
+
+The DB (60.4 GB for the three parties) is far larger than L2, so no L2 flush
+is needed between steps.  Synthetic seeded data (no dataset exists for this
+workload).  `--impl reference` times the CPU restatement of the reference's
+CPU path (per-party rotation-aware dots, summed, thresholded, OR over
+rotations) on the host cores.
+
+Multi-GPU (torchrun): each rank hosts its own 524,288-entry shard of all three
+parties and processes the same query batch; no data-path collective (weak
+scaling); the max step time over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "iris-mpc_b200")]
+
+METRIC = "iris comparisons/sec (3-party, 1 B200)"
+UNIT = "comparisons/s"
+DB_SEED = 0xDEADBEEF
+Q_SEED = 42
+K_CODE, K_MASK = 12800, 6400
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--db", type=int, default=524288, help="DB entries per party (per GPU)")
+    ap.add_argument("--queries", type=int, default=64)
+    ap.add_argument("--threshold-a", type=int, default=16384)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cublas", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(n_query=8, n_db=8192, min_seconds=10.0):
+    """The CPU restatement of the reference's CPU path on config 0's shape."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import oracle as O
+    import workload as W
+    O.build()
+    codes, masks, cs, ms = W.make_db(O, n_db, DB_SEED)
+    planted = {j: (int(j * 997 % n_db), (j % 31) - 15) for j in range(0, n_query, 10)}
+    qc, qm, _ = W.make_queries(O, n_query, codes, masks, Q_SEED, planted)
+    q_code = [W.rotated_rows(O, qc[p]) for p in range(3)]
+    q_mask = [W.rotated_rows(O, qm[p]) for p in range(3)]
+    cores = os.cpu_count() or 1
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.cpu_plain_match(q_code, q_mask, n_query, list(cs), list(ms), 16384, cores)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= 50:
+            break
+    value = reps * n_query * n_db / el
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n_query} queries x 31 rotations vs {n_db} entries, 3 parties, {reps} pass(es), "
+                      f"{el:.1f} s, OpenMP on {cores} threads"}
+
+
+def measure_int8_peak(torch):
+    """Dense INT8 denominator: cuBLAS int8 GEMM (torch._int_mm) 8192^3, best of 10."""
+    a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+    b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda").t()
+    for _ in range(3):
+        torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(10):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def cublas_limb_gemms(torch, m, n_rows, warm=2, reps=3):
+    """The reference's dot products on this GPU: per party, 3 cublasGemmEx int8
+    limb GEMMs for codes (K = 12800) and 3 for masks (K = 6400) via torch._int_mm
+    (share_db.rs:62-112,823-843).  Returns ms per batch for 3 parties."""
+    n = (n_rows + 7) // 8 * 8
+    out = {}
+    for k in (K_CODE, K_MASK):
+        a = torch.randint(-128, 127, (m, k), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (n, k), dtype=torch.int8, device="cuda").t()
+        for _ in range(warm):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            torch._int_mm(a, b)
+        e.record()
+        e.synchronize()
+        out[k] = s.elapsed_time(e) / reps
+        del a, b
+        torch.cuda.empty_cache()
+    per_party = 3 * out[K_CODE] + 3 * out[K_MASK]
+    return 3 * per_party
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_baseline()
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": "CPU plain method (reference CPU path restated in C, OpenMP): "
+                                   "3 parties in-process, 8 queries x 31 rotations vs 8192 entries",
+                       "threshold_ratio": 0.375},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import irisb200
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    M, NQ = args.db, args.queries
+    n_rows = NQ * 32
+    A = args.threshold_a
+    dm = irisb200.DeviceManager(local)
+    seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
+    ce = [irisb200.ShareDB(p, dm, M, n_rows, K_CODE, seeds[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, M, n_rows, K_MASK, seeds[p]) for p in range(3)]
+    for e in ce + me:
+        e.alloc_db(M)
+    t0 = time.perf_counter()
+    irisb200.synth_db(ce, me, DB_SEED + rank, 0, M)
+    synth_s = time.perf_counter() - t0
+    c = irisb200.Circuits(dm, seeds)
+    dc = irisb200.DistanceComparator(dm, NQ, M, match_list_cap=1 << 16)
+
+    # 10% of the queries are planted near-duplicates of DB entries of this shard
+    planted = {j: (int((j * 7919 + 13) % M), (j * 7) % 31 - 15) for j in range(0, NQ, 10)}
+    pin_c = irisb200.PinnedArray((3, NQ, K_CODE), np.uint16)
+    pin_m = irisb200.PinnedArray((3, NQ, K_MASK), np.uint16)
+    irisb200.synth_queries(DB_SEED + rank, Q_SEED, NQ, planted, code_out=pin_c.array, mask_out=pin_m.array)
+    slots = [(j, 0, 31, j) for j in range(NQ)]
+    engines = ce + me
+    mults = [1, 1, 1, 2, 2, 2]
+
+    def upload():
+        for p in range(3):
+            ce[p].query_upload_slots(pin_c.array[p], slots)
+            me[p].query_upload_slots(pin_m.array[p], slots)
+
+    s0 = torch.cuda.ExternalStream(dm.stream(0), device=torch.device("cuda", local))
+
+    def device_step(ev=None):
+        dc.reset()
+        if ev:
+            ev[0].record(s0)
+        irisb200.dot_many(engines, mults, 0, M)
+        if ev:
+            ev[1].record(s0)
+        dc.compare_threshold_open(c, ce, me, 0, M, NQ, A)
+        if ev:
+            ev[2].record(s0)
+
+    upload()
+    for _ in range(args.warmup):
+        device_step()
+    dm.synchronize()
+
+    # ---------------- device-resident timing ----------------
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    dm.synchronize()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        begin.record(s0)
+        for i in range(args.steps):
+            device_step(evs[i])
+        end.record(s0)
+        end.synchronize()
+    dm.synchronize()
+    total_ms = begin.elapsed_time(end)
+    step_ms = [evs[i][2].elapsed_time(evs[i + 1][2]) if i + 1 < args.steps else None for i in range(args.steps)]
+    gemm_ms = [evs[i][0].elapsed_time(evs[i][1]) for i in range(args.steps)]
+    thr_ms = [evs[i][1].elapsed_time(evs[i][2]) for i in range(args.steps)]
+    batch_ms = [evs[i][0].elapsed_time(evs[i][2]) for i in range(args.steps)]
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    per_step = total_ms / args.steps
+    comps = NQ * M * world
+    value = comps / (per_step * 1e-3)
+
+    # correctness guard on the measured run: the planted queries must match
+    dc.join_db_matches(NQ, M)
+    final, counters, _ = dc.fetch_final_results(NQ)
+    planted_found = sum(1 for j, (e, _) in planted.items() if final[j] <= e and counters[j] >= 1)
+
+    # ---------------- end-to-end timing through the public API ----------------
+    h2d = 3 * NQ * (K_CODE + K_MASK) * 2
+    d2h = NQ * 4 * 2 + NQ * irisb200.MAX_MATCHES_LEN * 4
+
+    def e2e_step():
+        upload()
+        dc.reset()
+        irisb200.dot_many(engines, mults, 0, M)
+        dc.compare_threshold_open(c, ce, me, 0, M, NQ, A)
+        dc.join_db_matches(NQ, M)
+        return dc.fetch_final_results(NQ)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    dm.synchronize()
+    lat = []
+    with ClockSampler(local) as clk_e2e:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ts = time.perf_counter()
+            e2e_step()
+            lat.append((time.perf_counter() - ts) * 1e3)
+        e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = comps * args.steps / e2e_s
+
+    result = None
+    if rank == 0:
+        ops = 3 * 6 * (K_CODE + K_MASK) * (NQ * 31) * M  # algorithmic int8 ops per GEMM launch
+        gemm_avg = statistics.mean(gemm_ms)
+        achieved = ops / (gemm_avg * 1e-3) / 1e12
+        peak = measure_int8_peak(torch)
+        cublas_ms = None if args.no_cublas else cublas_limb_gemms(torch, M, NQ * 31)
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "gemm_limb_traffic.json")
+        if os.path.exists(prof):
+            with open(prof) as f:
+                pj = json.load(f)
+            traffic = pj.get("bytes_per_launch_scaled")
+        lat_sorted = sorted(batch_ms)
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "GPU plain drop-in: 3 parties co-resident on one B200, 64 queries x 31 rotations "
+                                   "vs 524288 share-DB entries per party (per GPU)",
+                       "db_entries_per_party": M, "queries": NQ, "rotations": 31, "query_rows": NQ * 31,
+                       "padded_query_rows": n_rows, "threshold_a": A, "threshold_ratio": 0.375,
+                       "l2": "no flush: inputs (60.4 GB share DB) exceed the 126 MB L2",
+                       "parallelism": f"db-shard x{world}, 3 co-resident parties per GPU"},
+            "latency_ms": {"p50": lat_sorted[len(lat_sorted) // 2], "p99": lat_sorted[-1],
+                           "e2e_p50": sorted(lat)[len(lat) // 2], "e2e_p99": max(lat)},
+            "kernels_ms": {"limb_gemm_6_engines": gemm_avg, "threshold_open_or": statistics.mean(thr_ms)},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "limb_gemm_kernel<256> (6 engines, one launch)",
+                         "ops_per_launch": ops,
+                         "peak_source": "dense INT8 measured in this run: cuBLAS int8 GEMM (torch._int_mm) "
+                                        "8192^3, best of 10",
+                         "frac_of_2x_bf16_measured": None},
+            "cublas_limb_gemm_ms_per_batch": cublas_ms,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": 2 * args.steps,
+            "gpu_launches_e2e": 9 * args.steps,
+            "clocks": clk.summary(),
+            "clocks_e2e": clk_e2e.summary(),
+            "planted_matches_found": f"{planted_found}/{len(planted)}",
+            "setup_s": {"synth_db": synth_s},
+        }
+        mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(mp):
+            with open(mp) as f:
+                bf16 = json.load(f).get("bf16_tflops")
+            if bf16:
+                result["roofline"]["frac_of_2x_bf16_measured"] = achieved / (2 * bf16)
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(result), flush=True)
+
+    for o in ce + me + [c, dc]:
+        o.close()
+    dm.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

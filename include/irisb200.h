@@ -70,6 +70,9 @@ int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
 
 /* Plain device memory helpers for callers that stage their own buffers. */
 int irs_device_alloc(irs_device_manager* dm, size_t bytes, void** ptr);
+/* Page-locked host memory (register_host_memory, device_manager.rs:214-238). */
+int irs_host_alloc_pinned(size_t bytes, void** ptr);
+int irs_host_free_pinned(void* ptr);
 int irs_device_free(irs_device_manager* dm, void* ptr);
 int irs_copy_h2d(void* dst, const void* src, size_t bytes, void* stream);
 int irs_copy_d2h(void* dst, const void* src, size_t bytes, void* stream);
@@ -110,6 +113,20 @@ int irs_sharedb_db_len(irs_sharedb* db, size_t* len);
  * the seeded synthetic irises of the benchmark workload (device-side). */
 int irs_sharedb_synth_db(irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3], uint64_t seed,
                          size_t first, size_t n);
+
+/* preprocess_iris_code_query_share / preprocess_mask_code_query_share
+ * (galois_engine.rs:23-40,193-195,438-440) on the host, in place: each GR4
+ * block times the party's Lagrange coefficient at 0, converted to basis B. */
+int irs_preprocess_query_share(int party, uint16_t* coefs, size_t n);
+
+/* Seeded synthetic queries of the benchmark workload (host): query j is a
+ * near-duplicate of DB entry planted_entry[j] (code bits flipped with p = 0.2,
+ * rotated by planted_rot[j] columns) or, for planted_entry[j] < 0, a fresh
+ * iris.  Writes the three parties' shares, code_out [3][n_queries][12800] and
+ * mask_out [3][n_queries][6400] (trimmed), preprocessed when `preprocess`.
+ * The DB entries are those irs_sharedb_synth_db generates for db_seed. */
+int irs_synth_queries(uint64_t db_seed, uint64_t q_seed, size_t n_queries, const int64_t* planted_entry,
+                      const int32_t* planted_rot, int preprocess, uint16_t* code_out, uint16_t* mask_out);
 
 /* Query upload: preprocess_query + htod_transfer_query
  * (share_db.rs:45-59; device_manager.rs:159-212), rows given as-is

@@ -240,6 +240,21 @@ int irs_device_alloc(irs_device_manager* dm, size_t bytes, void** ptr) {
   return IRS_OK;
 }
 
+int irs_host_alloc_pinned(size_t bytes, void** ptr) {
+  CHECK(ptr, IRS_ERR_INVALID, "ptr is NULL");
+  cudaError_t e = cudaMallocHost(ptr, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(IRS_ERR_NOMEM, "cudaMallocHost(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  return IRS_OK;
+}
+
+int irs_host_free_pinned(void* ptr) {
+  if (ptr) CU(cudaFreeHost(ptr));
+  return IRS_OK;
+}
+
 int irs_device_free(irs_device_manager* dm, void* ptr) {
   (void)dm;
   if (ptr) CU(cudaFree(ptr));

@@ -59,6 +59,10 @@ _SIGS = {
     "irs_device_manager_sm_count": [_vp, C.POINTER(_i)],
     "irs_device_alloc": [_vp, _sz, C.POINTER(_vp)],
     "irs_device_free": [_vp, _vp],
+    "irs_host_alloc_pinned": [_sz, C.POINTER(_vp)],
+    "irs_host_free_pinned": [_vp],
+    "irs_preprocess_query_share": [_i, _vp, _sz],
+    "irs_synth_queries": [_u64, _u64, _sz, _vp, _vp, _i, _vp, _vp],
     "irs_copy_h2d": [_vp, _vp, _sz, _vp],
     "irs_copy_d2h": [_vp, _vp, _sz, _vp],
     "irs_stream_synchronize": [_vp],
@@ -172,6 +176,56 @@ class DeviceBuffer:
             self.free()
         except Exception:
             pass
+
+
+class PinnedArray:
+    """A numpy array over page-locked host memory (cudaMallocHost)."""
+
+    def __init__(self, shape, dtype):
+        dtype = np.dtype(dtype)
+        n = int(np.prod(shape)) * dtype.itemsize
+        p = _vp()
+        _check(lib().irs_host_alloc_pinned(n, C.byref(p)))
+        self._p = p.value
+        buf = (C.c_uint8 * n).from_address(self._p)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self) -> None:
+        if self._p:
+            self.array = None
+            lib().irs_host_free_pinned(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def preprocess_query_share(party: int, coefs: np.ndarray) -> np.ndarray:
+    """Lagrange x basis-B preprocessing of a query share (galois_engine.rs:23-40)."""
+    out = np.ascontiguousarray(coefs, np.uint16).copy()
+    _check(lib().irs_preprocess_query_share(party, _ptr(out), out.size))
+    return out
+
+
+def synth_queries(db_seed: int, q_seed: int, n_queries: int, planted: dict, preprocess: bool = True,
+                  code_out: np.ndarray = None, mask_out: np.ndarray = None):
+    """Seeded synthetic query shares; planted = {query: (db entry, rotation)}.
+    Returns (code [3][n][12800], mask [3][n][6400]) u16."""
+    pe = np.full(n_queries, -1, np.int64)
+    pr = np.zeros(n_queries, np.int32)
+    for j, (e, r) in planted.items():
+        pe[j] = e
+        pr[j] = r
+    code = code_out if code_out is not None else np.zeros((3, n_queries, IRIS_CODE_LENGTH), np.uint16)
+    mask = mask_out if mask_out is not None else np.zeros((3, n_queries, MASK_CODE_LENGTH), np.uint16)
+    assert code.shape == (3, n_queries, IRIS_CODE_LENGTH) and code.flags.c_contiguous
+    assert mask.shape == (3, n_queries, MASK_CODE_LENGTH) and mask.flags.c_contiguous
+    _check(lib().irs_synth_queries(db_seed, q_seed, n_queries, _ptr(pe), _ptr(pr), int(preprocess), _ptr(code),
+                                   _ptr(mask)))
+    return code, mask
 
 
 class DeviceManager:
