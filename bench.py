@@ -69,8 +69,9 @@ class ClockSampler:
 
     def __init__(self, index: int):
         self.index = index
-        self.lines = []
+        self.lines = []  # (host time, csv line)
         self.proc = None
+        self.windows = []
 
     def __enter__(self):
         try:
@@ -85,7 +86,20 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self):
+        """Context manager recording a timed window; summaries use samples inside windows."""
+        sampler = self
+
+        class _W:
+            def __enter__(self_):
+                self_.t0 = time.perf_counter()
+                return self_
+
+            def __exit__(self_, *exc):
+                sampler.windows.append((self_.t0, time.perf_counter()))
+        return _W()
 
     def __exit__(self, *exc):
         if self.proc:
@@ -95,10 +109,13 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, window=None):
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lo, hi = window if window else (float("-inf"), float("inf"))
+        for t, ln in self.lines:
+            if not (lo <= t <= hi + 0.25):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -140,10 +157,10 @@ def cpu_baseline(n_query=8, n_db=8192, min_seconds=10.0):
                       f"{el:.1f} s, OpenMP on {cores} threads"}
 
 
-def measure_int8_peak(torch):
-    """Dense INT8 denominator: cuBLAS int8 GEMM (torch._int_mm) 8192^3, best of 10."""
-    a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
-    b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda").t()
+def measure_int8_peak(torch, n=16384):
+    """Dense INT8 denominator: cuBLAS int8 GEMM (torch._int_mm) n^3, best of 10."""
+    a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda").t()
     for _ in range(3):
         torch._int_mm(a, b)
     torch.cuda.synchronize()
@@ -156,7 +173,7 @@ def measure_int8_peak(torch):
         e.synchronize()
         best = min(best, s.elapsed_time(e))
     del a, b
-    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
 
 
 def cublas_limb_gemms(torch, m, n_rows, warm=2, reps=3):
@@ -259,6 +276,8 @@ def run_ours(args):
         if ev:
             ev[2].record(s0)
 
+    clk = ClockSampler(local).__enter__()
+    time.sleep(2.0)  # let nvidia-smi initialise before anything is timed
     upload()
     for _ in range(args.warmup):
         device_step()
@@ -271,7 +290,7 @@ def run_ours(args):
         dist.barrier()
     dm.synchronize()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    with clk.mark():
         begin.record(s0)
         for i in range(args.steps):
             device_step(evs[i])
@@ -314,13 +333,14 @@ def run_ours(args):
         dist.barrier()
     dm.synchronize()
     lat = []
-    with ClockSampler(local) as clk_e2e:
+    with clk.mark():
         t0 = time.perf_counter()
         for _ in range(args.steps):
             ts = time.perf_counter()
             e2e_step()
             lat.append((time.perf_counter() - ts) * 1e3)
         e2e_s = time.perf_counter() - t0
+    clk.__exit__(None, None, None)
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -359,14 +379,14 @@ def run_ours(args):
                          "kernel": "limb_gemm_kernel<256> (6 engines, one launch)",
                          "ops_per_launch": ops,
                          "peak_source": "dense INT8 measured in this run: cuBLAS int8 GEMM (torch._int_mm) "
-                                        "8192^3, best of 10",
+                                        "16384^3, best of 10",
                          "frac_of_2x_bf16_measured": None},
             "cublas_limb_gemm_ms_per_batch": cublas_ms,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * args.steps,
             "gpu_launches_e2e": 9 * args.steps,
-            "clocks": clk.summary(),
-            "clocks_e2e": clk_e2e.summary(),
+            "clocks": clk.summary(clk.windows[0]),
+            "clocks_e2e": clk.summary(clk.windows[1]),
             "planted_matches_found": f"{planted_found}/{len(planted)}",
             "setup_s": {"synth_db": synth_s},
         }

@@ -50,6 +50,19 @@ IRS_HD Comp cand(Comp x, Comp y, uint32_t k0, uint32_t k1, uint32_t k2) {
   return z;
 }
 
+// Block `counter` of the three streams into ks[3][16].  Kept out of line: the
+// circuit draws 24 blocks per word, and one shared copy of the ChaCha code
+// keeps the kernel's instruction working set inside the instruction cache.
+#ifdef __CUDACC__
+__host__ __device__ __noinline__
+#else
+static
+#endif
+void chacha12_x3(const ChaChaKey* key, uint64_t counter, uint64_t nonce, uint32_t* ks) {
+#pragma unroll 1
+  for (int s = 0; s < 3; s++) chacha_block<12>(key[s], counter, nonce, ks + 16 * s);
+}
+
 // Keystream of one word: the current block of each of the three streams.
 struct WordRand {
   ChaChaKey key[3];
@@ -59,9 +72,7 @@ struct WordRand {
   int block;
   IRS_HD void load(int b) {
     block = b;
-    chacha_block<12>(key[0], base + (uint64_t)b, nonce, ks[0]);
-    chacha_block<12>(key[1], base + (uint64_t)b, nonce, ks[1]);
-    chacha_block<12>(key[2], base + (uint64_t)b, nonce, ks[2]);
+    chacha12_x3(key, base + (uint64_t)b, nonce, &ks[0][0]);
   }
 };
 

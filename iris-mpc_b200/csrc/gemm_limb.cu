@@ -133,6 +133,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Keystream blocks of the party's own and previous seed at one counter; out of
+// line so the epilogue carries a single copy of the ChaCha code.
+__device__ __noinline__ void chacha12_pair(const ChaChaKey* own, const ChaChaKey* prev, uint64_t counter,
+                                           uint64_t nonce, uint32_t* out /* [32] */) {
+  chacha_block<12>(*own, counter, nonce, out);
+  chacha_block<12>(*prev, counter, nonce, out + 16);
+}
+
 template <int BN>
 struct Cfg {
   static constexpr int kStageBytes = 2 * kBM * kBK + 2 * BN * kBK;
@@ -320,11 +328,10 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
           }
           if (pr.mask_on) {
             const uint64_t blk = (m_global * pr.n_pad + n) >> 5;
-            uint32_t ko[16], kp[16];
-            chacha_block<12>(pr.key_own, counter_of(pr.batch, blk), pr.nonce, ko);
-            chacha_block<12>(pr.key_prev, counter_of(pr.batch, blk), pr.nonce, kp);
+            uint32_t ks[32];
+            chacha12_pair(&pr.key_own, &pr.key_prev, counter_of(pr.batch, blk), pr.nonce, ks);
 #pragma unroll
-            for (int j = 0; j < 16; j++) v[j] = sub2(add2(v[j], ko[j]), kp[j]);
+            for (int j = 0; j < 16; j++) v[j] = sub2(add2(v[j], ks[j]), ks[16 + j]);
           }
           uint4* dst = reinterpret_cast<uint4*>(out_row + n);
 #pragma unroll

@@ -20,6 +20,7 @@
 //             with one ballot per warp, and matches are appended to a list.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include "circuit.cuh"
 #include "threshold.h"
 
@@ -54,7 +55,8 @@ __global__ void __launch_bounds__(kThreshThreads) threshold_flat_kernel(const Th
   }
 }
 
-__global__ void __launch_bounds__(kThreshThreads) threshold_bitmap_kernel(const ThresholdParams P) {
+template <int MIN_BLOCKS>
+__global__ void __launch_bounds__(kThreshThreads, MIN_BLOCKS) threshold_bitmap_kernel(const ThresholdParams P) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t n_groups = (P.n_entries + 31) / 32;
@@ -130,7 +132,16 @@ cudaError_t launch_threshold_bitmap(const ThresholdParams& P, cudaStream_t strea
   const uint64_t warps = (uint64_t)((P.n_entries + 31) / 32) * P.n_slots;
   const uint64_t threads = warps * 32;
   const unsigned grid = (unsigned)((threads + kThreshThreads - 1) / kThreshThreads);
-  threshold_bitmap_kernel<<<grid, kThreshThreads, 0, stream>>>(P);
+  // Occupancy variant (blocks of 128 threads per SM the registers are sized
+  // for); IRS_THRESHOLD_MIN_BLOCKS overrides the default for tuning runs.
+  static int min_blocks = [] {
+    const char* e = getenv("IRS_THRESHOLD_MIN_BLOCKS");
+    const int v = e ? atoi(e) : 2;
+    return (v == 3 || v == 4) ? v : 2;
+  }();
+  if (min_blocks == 4) threshold_bitmap_kernel<4><<<grid, kThreshThreads, 0, stream>>>(P);
+  else if (min_blocks == 3) threshold_bitmap_kernel<3><<<grid, kThreshThreads, 0, stream>>>(P);
+  else threshold_bitmap_kernel<2><<<grid, kThreshThreads, 0, stream>>>(P);
   return cudaGetLastError();
 }
 
