@@ -193,6 +193,23 @@ int irs_circuits_compare_threshold_masked_many(irs_circuits* c, const uint16_t* 
                                                const uint16_t* const mask_a[3], size_t n, uint32_t threshold_a,
                                                uint64_t* const res_a[3], uint64_t* const res_b[3], uint64_t* opened,
                                                void* stream);
+/* compare_threshold_masked_many for callers that cannot allocate device
+ * memory after start-up (e.g. a server that reserved all of HBM for the share
+ * database, or a host runtime whose own allocator owns the device).  No
+ * counterpart in the reference.  Same arguments and results as
+ * irs_circuits_compare_threshold_masked_many, but its scratch lives in a
+ * static device array of IRS_NOALLOC_MAX_ELEMENTS / 32 words per party that
+ * every GPU loading the library holds until exit; it calls no allocator.
+ * n above IRS_NOALLOC_MAX_ELEMENTS is rejected with IRS_ERR_INVALID.  The
+ * first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array: calls whose work overlaps on the GPU race and must be
+ * serialised by the caller. */
+#define IRS_NOALLOC_MAX_ELEMENTS (1u << 22)
+int irs_circuits_compare_threshold_masked_many_noalloc(irs_circuits* c, const uint16_t* const code_a[3],
+                                                       const uint16_t* const mask_a[3], size_t n,
+                                                       uint32_t threshold_a, uint64_t* const res_a[3],
+                                                       uint64_t* const res_b[3], uint64_t* opened, void* stream);
 /* lift_mul_sub + extract_msb with the lifted mask at zero
  * (tests/extract_msb_mod.rs:180-215): msb of -code*2^16 - 1. */
 int irs_circuits_extract_msb_of_code(irs_circuits* c, const uint16_t* const code_a[3], size_t n,

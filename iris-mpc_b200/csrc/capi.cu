@@ -18,6 +18,7 @@
 #include "../../include/irisb200.h"
 #include "common.cuh"
 #include "gemm_limb.h"
+#include "internal.h"
 #include "prep.h"
 #include "results.h"
 #include "threshold.h"
@@ -973,3 +974,28 @@ int irs_dc_fetch_final_results(irs_distance_comparator* dc, size_t n_queries, ui
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Internal accessors (internal.h)
+// ---------------------------------------------------------------------------
+namespace irs {
+
+int set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int circuit_view(irs_circuits* c, CircuitView* v) {
+  if (!c || !v) return set_error(IRS_ERR_INVALID, "circuits handle is NULL");
+  for (int p = 0; p < 3; p++) v->keys[p] = c->keys[p];
+  v->nonce = nonce_of(kDomCircuit, (uint32_t)c->dm->device);
+  v->batch = c->batch;
+  v->device = c->dm->device;
+  v->stream0 = c->dm->streams[0];
+  return IRS_OK;
+}
+
+}  // namespace irs

@@ -86,6 +86,7 @@ _SIGS = {
     "irs_circuits_destroy": [_vp],
     "irs_circuits_set_batch": [_vp, _u64],
     "irs_circuits_compare_threshold_masked_many": [_vp, _vp, _vp, _sz, _u32, _vp, _vp, _vp, _vp],
+    "irs_circuits_compare_threshold_masked_many_noalloc": [_vp, _vp, _vp, _sz, _u32, _vp, _vp, _vp, _vp],
     "irs_circuits_extract_msb_of_code": [_vp, _vp, _sz, _vp, _vp, _vp, _vp],
     "irs_circuits_lift_mpc": [_vp, _vp, _sz, _vp, _vp],
     "irs_dc_init": [_vp, _sz, _sz, _sz, C.POINTER(_vp)],
