@@ -320,8 +320,10 @@ int irs_sharedb_init(irs_device_manager* dm, int peer_id, size_t max_db_length, 
   db->d_slots = (QuerySlot*)p;
   if ((rc = pool_alloc(dm, peer_id, max_db_length * db->n_pad * 2, &p))) { irs_sharedb_destroy(db); return rc; }
   db->results = (uint16_t*)p;
-  if (make_tmap_u8(&db->tm_q_lo, db->q_lo, db->n_pad, code_length, (uint32_t)db->block_n) ||
-      make_tmap_u8(&db->tm_q_hi, db->q_hi, db->n_pad, code_length, (uint32_t)db->block_n)) {
+  // The two-SM GEMM loads half of a query tile per CTA.
+  const uint32_t q_box = (uint32_t)(gemm_use_pair(db->block_n) ? db->block_n / 2 : db->block_n);
+  if (make_tmap_u8(&db->tm_q_lo, db->q_lo, db->n_pad, code_length, q_box) ||
+      make_tmap_u8(&db->tm_q_hi, db->q_hi, db->n_pad, code_length, q_box)) {
     irs_sharedb_destroy(db);
     return fail(IRS_ERR_CUDA, "tensor map for the query planes failed");
   }

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include "common.cuh"
 #include "gemm_limb.h"
 
@@ -349,6 +350,290 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
   }
 }
 
+// ---------------------------------------------------------------------------
+// Two-SM variant: a cluster of two CTAs computes a 256-entry x 256-row tile
+// with tcgen05.mma.cta_group::2 (M = 256).  Each CTA loads its own 128 entries
+// (A) and half of the 256 query rows (B); the leader CTA (rank 0) issues the
+// MMAs, which read the A and B halves from both CTAs' shared memory, and each
+// CTA's TMEM receives the accumulator rows of its own entries.  Per SM this
+// halves the B bytes written into and read from shared memory, which is what
+// bounds the one-SM kernel (about 156 of 128 B/clk at full MMA rate).
+// TMA completions of both CTAs land on the leader's stage barriers; stage and
+// accumulator barriers are released to both CTAs with multicast commits; the
+// follower's epilogue releases the accumulator on the leader's barrier.
+// ---------------------------------------------------------------------------
+constexpr int kBM2 = 256;
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ uint32_t map_to_rank(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster_addr, int x,
+                                                 int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster_addr)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_u8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
+
+// Arrives on the barrier at the same offset in both CTAs of the pair once the
+// leader's preceding MMAs have completed.
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar) {
+  const uint16_t mask = 0x3;
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"(mask)
+      : "memory");
+}
+
+__host__ __device__ constexpr uint32_t idesc_u8_m256(int bn) {
+  return (2u << 4) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(kBM2 >> 4) << 24);
+}
+
+struct Cfg2 {
+  static constexpr int BN = 256;
+  static constexpr int kHalfN = BN / 2;
+  static constexpr int kStageBytes = 2 * 128 * kBK + 2 * kHalfN * kBK;  // per CTA
+  static constexpr int kStages = 3;
+  static constexpr int kTmemCols = 2 * BN;
+  static constexpr int kColsPerThread = BN / 2;
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
+};
+
+__device__ __forceinline__ bool tile_of2(const GemmParams& P, int t, Tile& out) {
+  for (int i = 0; i < P.n_prob; i++) {
+    const int nt = (int)(P.prob[i].tiles_m * P.prob[i].tiles_n);
+    if (t < nt) {
+      out.prob = i;
+      out.m_tile = t / (int)P.prob[i].tiles_n;
+      out.n_tile = t % (int)P.prob[i].tiles_n;
+      return true;
+    }
+    t -= nt;
+  }
+  return false;
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    limb_gemm_pair_kernel(const __grid_constant__ GemmParams P) {
+  using C = Cfg2;
+  constexpr int BN = C::BN;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* a_lo = smem;
+  uint8_t* a_hi = a_lo + C::kStages * 128 * kBK;
+  uint8_t* b_lo = a_hi + C::kStages * 128 * kBK;
+  uint8_t* b_hi = b_lo + C::kStages * C::kHalfN * kBK;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(b_hi + C::kStages * C::kHalfN * kBK);
+  uint64_t* full_bar = bars;
+  uint64_t* empty_bar = bars + C::kStages;
+  uint64_t* acc_full = bars + 2 * C::kStages;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* done_bar = acc_full + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 3);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const int cluster = blockIdx.x >> 1;
+  const int n_clusters = gridDim.x >> 1;
+  int* err = P.err;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::kStages; s++) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 16);  // 8 epilogue warps in each CTA
+    mbar_init(done_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)C::kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // peer barriers initialised before any remote arrive
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int issued_phase[C::kStages];
+      bool issued[C::kStages];
+      for (int s = 0; s < C::kStages; s++) issued[s] = false;
+      bool ok = true;
+      for (int t = cluster; ok && t < P.total_tiles; t += n_clusters) {
+        Tile tl;
+        if (!tile_of2(P, t, tl)) break;
+        const GemmProblem& pr = P.prob[tl.prob];
+        const int ya = (int)pr.m0 + tl.m_tile * kBM2 + (int)rank * 128;
+        const int yb = tl.n_tile * BN + (int)rank * C::kHalfN;
+        for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1u, err, kErrTimeoutEmpty)) { ok = false; break; }
+          if (leader) mbar_expect_tx(&full_bar[stage], (uint32_t)(2 * C::kStageBytes));
+          const uint32_t fb = map_to_rank(&full_bar[stage], 0);
+          const int x = (int)ki * kBK;
+          tma_load_2d_pair(a_lo + stage * 128 * kBK, &pr.tm_a_lo, fb, x, ya);
+          tma_load_2d_pair(a_hi + stage * 128 * kBK, &pr.tm_a_hi, fb, x, ya);
+          tma_load_2d_pair(b_lo + stage * C::kHalfN * kBK, &pr.tm_b_lo, fb, x, yb);
+          tma_load_2d_pair(b_hi + stage * C::kHalfN * kBK, &pr.tm_b_hi, fb, x, yb);
+          issued[stage] = true;
+          issued_phase[stage] = (int)phase;
+          if (++stage == C::kStages) { stage = 0; phase ^= 1u; }
+        }
+      }
+      // Exit: the leader's stage barriers complete only when both CTAs' copies
+      // of that stage have landed.
+      if (leader)
+        for (int s = 0; s < C::kStages; s++)
+          if (issued[s]) mbar_wait(&full_bar[s], (uint32_t)issued_phase[s], err, kErrTimeoutDrain);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (leader CTA only) ----------------
+    if (lane == 0 && leader) {
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t acc_phase = 0;
+      bool ok = true;
+      constexpr uint32_t idesc = idesc_u8_m256(BN);
+      for (int t = cluster; ok && t < P.total_tiles; t += n_clusters) {
+        Tile tl;
+        if (!tile_of2(P, t, tl)) break;
+        const GemmProblem& pr = P.prob[tl.prob];
+        if (!mbar_wait(acc_empty, acc_phase ^ 1u, err, kErrTimeoutAccEmpty)) { ok = false; break; }
+        acc_phase ^= 1u;
+        tc_fence_after();
+        for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
+          if (!mbar_wait(&full_bar[stage], phase, err, kErrTimeoutFull)) { ok = false; break; }
+          tc_fence_after();
+          const uint64_t dal = smem_desc(a_lo + stage * 128 * kBK);
+          const uint64_t dah = smem_desc(a_hi + stage * 128 * kBK);
+          const uint64_t dbl = smem_desc(b_lo + stage * C::kHalfN * kBK);
+          const uint64_t dbh = smem_desc(b_hi + stage * C::kHalfN * kBK);
+#pragma unroll
+          for (int kk = 0; kk < kBK / 32; kk++) {
+            const uint32_t acc = (ki > 0 || kk > 0) ? 1u : 0u;
+            const uint64_t o = (uint64_t)(2 * kk);
+            mma_u8_pair(tmem, dal + o, dbl + o, idesc, acc);
+            mma_u8_pair(tmem + BN, dal + o, dbh + o, idesc, acc);
+            mma_u8_pair(tmem + BN, dah + o, dbl + o, idesc, 1u);
+          }
+          mma_commit_pair(&empty_bar[stage]);
+          if (++stage == C::kStages) { stage = 0; phase ^= 1u; }
+        }
+        if (ok) mma_commit_pair(acc_full);
+      }
+      asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(done_bar))
+                   : "memory");
+      mbar_wait(done_bar, 0, err, kErrTimeoutDrain);
+    }
+  } else {
+    // ---------------- Epilogue (warps 2..9, both CTAs) ----------------
+    const int quad = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int row = quad * 32 + lane;
+    constexpr int kCols = C::kColsPerThread;
+    const uint32_t acc_empty_leader = map_to_rank(acc_empty, 0);
+    uint32_t acc_phase = 0;
+    for (int t = cluster; t < P.total_tiles; t += n_clusters) {
+      Tile tl;
+      if (!tile_of2(P, t, tl)) break;
+      const GemmProblem& pr = P.prob[tl.prob];
+      if (!mbar_wait(acc_full, acc_phase, err, kErrTimeoutAccFull)) break;
+      acc_phase ^= 1u;
+      tc_fence_after();
+      uint32_t packed[kCols / 2];
+      const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(half * kCols);
+#pragma unroll
+      for (int c = 0; c < kCols / 32; c++) {
+        uint32_t r0[32], r1[32];
+        tmem_ld32(tbase + (uint32_t)(c * 32), r0);
+        tmem_ld32(tbase + (uint32_t)(BN + c * 32), r1);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const uint32_t lo = (r0[2 * j] + (r1[2 * j] << 8)) & 0xFFFFu;
+          const uint32_t hi = (r0[2 * j + 1] + (r1[2 * j + 1] << 8)) << 16;
+          packed[c * 16 + j] = lo | hi;
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(acc_empty_leader);
+
+      const uint32_t m_local = (uint32_t)(tl.m_tile * kBM2 + (int)rank * 128 + row);
+      if (m_local < pr.m_len) {
+        const uint64_t m_global = (uint64_t)pr.m0 + m_local;
+        uint16_t* out_row = pr.out + (size_t)m_local * pr.n_pad;
+#pragma unroll
+        for (int c = 0; c < kCols / 32; c++) {
+          const uint32_t n = (uint32_t)(tl.n_tile * BN + half * kCols + c * 32);
+          uint32_t v[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const uint32_t x = packed[c * 16 + j];
+            v[j] = (pr.mult == 1) ? x : (((x & 0xFFFFu) * pr.mult) & 0xFFFFu) | (((x >> 16) * pr.mult) << 16);
+          }
+          if (pr.mask_on) {
+            const uint64_t blk = (m_global * pr.n_pad + n) >> 5;
+            uint32_t ks[32];
+            chacha12_pair(&pr.key_own, &pr.key_prev, counter_of(pr.batch, blk), pr.nonce, ks);
+#pragma unroll
+            for (int j = 0; j < 16; j++) v[j] = sub2(add2(v[j], ks[j]), ks[16 + j]);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(out_row + n);
+#pragma unroll
+          for (int q = 0; q < 4; q++) dst[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // no CTA leaves while its peer may still touch its memory
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)C::kTmemCols));
+  }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -398,6 +683,28 @@ static cudaError_t launch_bn(const GemmParams& P, int n_sms, cudaStream_t stream
   return cudaGetLastError();
 }
 
+static cudaError_t launch_pair(const GemmParams& P, int n_sms, cudaStream_t stream) {
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(limb_gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Cfg2::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  const int clusters = P.total_tiles < n_sms / 2 ? P.total_tiles : n_sms / 2;
+  if (clusters <= 0) return cudaSuccess;
+  limb_gemm_pair_kernel<<<2 * clusters, kThreads, Cfg2::kSmemBytes, stream>>>(P);
+  return cudaGetLastError();
+}
+
+bool gemm_use_pair(int block_n) {
+  static const bool enabled = [] {
+    const char* e = getenv("IRS_GEMM_PAIR");
+    return !(e && e[0] == '0');
+  }();
+  return enabled && block_n == 256;
+}
+
 int gemm_block_n_for(uint32_t n_pad) {
   if (n_pad % 256 == 0) return 256;
   if (n_pad % 128 == 0) return 128;
@@ -406,13 +713,16 @@ int gemm_block_n_for(uint32_t n_pad) {
 }
 
 cudaError_t launch_limb_gemm(GemmParams& P, int block_n, int n_sms, cudaStream_t stream) {
+  const bool pair = gemm_use_pair(block_n);
+  const uint32_t bm = pair ? (uint32_t)kBM2 : (uint32_t)kBM;
   P.total_tiles = 0;
   for (int i = 0; i < P.n_prob; i++) {
     GemmProblem& pr = P.prob[i];
-    pr.tiles_m = (pr.m_len + kBM - 1) / kBM;
+    pr.tiles_m = (pr.m_len + bm - 1) / bm;
     pr.tiles_n = pr.n_pad / (uint32_t)block_n;
     P.total_tiles += (int)(pr.tiles_m * pr.tiles_n);
   }
+  if (pair) return launch_pair(P, n_sms, stream);
   switch (block_n) {
     case 256: return launch_bn<256>(P, n_sms, stream);
     case 128: return launch_bn<128>(P, n_sms, stream);
