@@ -697,10 +697,14 @@ static cudaError_t launch_pair(const GemmParams& P, int n_sms, cudaStream_t stre
   return cudaGetLastError();
 }
 
+// The pair kernel reaches a higher MAC rate per clock but, at the B200's
+// 1000 W limit, pulls the SM clock down further than it gains (measured: about
+// 1000 MHz against 1500 MHz for the one-SM kernel, 17% fewer comparisons/s per
+// batch), so it is opt-in: IRS_GEMM_PAIR=1.
 bool gemm_use_pair(int block_n) {
   static const bool enabled = [] {
     const char* e = getenv("IRS_GEMM_PAIR");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
   }();
   return enabled && block_n == 256;
 }

@@ -47,7 +47,7 @@ int gemm_block_n_for(uint32_t n_pad);
 
 // True when launch_limb_gemm runs the two-SM (cta_group::2) kernel for this
 // tile width; its query tensor maps must then use boxes of block_n / 2 rows.
-// IRS_GEMM_PAIR=0 selects the one-SM kernel (tuning runs).
+// Off unless IRS_GEMM_PAIR=1 (the one-SM kernel is faster under the power cap).
 bool gemm_use_pair(int block_n);
 
 cudaError_t launch_limb_gemm(GemmParams& P, int block_n, int n_sms, cudaStream_t stream);
