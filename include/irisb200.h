@@ -65,6 +65,11 @@ int irs_device_manager_synchronize(irs_device_manager* dm);
 /* Device error word: 0, or the code of the first bounded wait that expired. */
 int irs_device_manager_error(irs_device_manager* dm, int* code);
 int irs_device_manager_clear_error(irs_device_manager* dm);
+/* Device-resident batch counter: engines and circuits switched to it with
+ * irs_sharedb_use_batch_counter / irs_circuits_use_batch_counter read their
+ * ChaCha batch id from device memory at run time, so a captured graph can be
+ * replayed for every batch with a fresh counter (set here, outside capture). */
+int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_id, void* stream);
 /* Number of SMs the persistent kernels size their grids to. */
 int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
 
@@ -147,6 +152,24 @@ typedef struct irs_query_slot {
  * the rotations on the device into 32-row slots (row 32*s + r). */
 int irs_sharedb_query_upload_slots(irs_sharedb* db, const uint16_t* base, size_t n_base,
                                    const irs_query_slot* slots, size_t n_slots);
+/* Uploads preprocessed base queries [n_base][code_length] and fills query row
+ * r with row_desc[r] = (src << 8) | rotation (rotation 0..30 of base query src,
+ * 15 = centre), 0xFFFFFFFF = zero row.  Packs queries with any rotation count
+ * densely (the batched launch of uneven requests). */
+int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t n_base, const uint32_t* row_desc,
+                                  size_t n_rows);
+/* prefetch_subset (share_db.rs:344-407), device to device: copies DB records
+ * ids[k] of `src` into records k of `dst` (same party and code length) and
+ * sets dst's length to n.  Used for reauth targets and subset re-checks. */
+int irs_sharedb_gather_records(irs_sharedb* dst, irs_sharedb* src, const uint32_t* ids, size_t n);
+/* mirrored_code / mirrored_mask (galois_engine.rs:218-225,520-543) of a
+ * (preprocessed or raw) query share, in place; flip_imaginary = 1 for codes. */
+int irs_mirror_query_share(uint16_t* coefs, size_t n, int flip_imaginary);
+/* Tile width of the dot kernel along the query rows: 64, 128 or 256, or 0 for
+ * the widest that divides the padded row count (the batch autotuner's knob).
+ * The padded row count of a batch is its uploaded rows rounded up to 64. */
+int irs_sharedb_set_tile(irs_sharedb* db, int block_n);
+int irs_sharedb_use_batch_counter(irs_sharedb* db, int on);
 /* Starts a new batch: the zero-share mask and circuit keystreams are drawn at
  * ChaCha counter (batch_id << 40) | position (ChaChaCtx counter,
  * iris-mpc-gpu/src/rng/chacha.rs:205-250). */
@@ -182,6 +205,7 @@ typedef struct irs_circuits irs_circuits;
 int irs_circuits_new(irs_device_manager* dm, const uint32_t seeds[3][2][8], irs_circuits** out);
 int irs_circuits_destroy(irs_circuits* c);
 int irs_circuits_set_batch(irs_circuits* c, uint64_t batch_id);
+int irs_circuits_use_batch_counter(irs_circuits* c, int on);
 
 /* compare_threshold_masked_many (protocol.rs:2519-2546) on n elements
  * (multiple of 64).  code_a[p]/mask_a[p]: party p's own u16 share (device);
@@ -246,6 +270,18 @@ int irs_dc_compare_threshold_open(irs_distance_comparator* dc, irs_circuits* c, 
                                   irs_sharedb* const mask_engines[3], size_t offset, size_t len, size_t n_slots,
                                   const uint32_t* slot_valid, const uint32_t* slot_query, uint32_t threshold_a,
                                   int self_check, void* stream);
+/* Segment table for packed query rows: slot s (32 rows) holds segments
+ * seg_start[s] .. seg_start[s+1]-1; segment k ORs the opened bits of rows
+ * seg_mask[k] into bitmap row seg_query[k].  Copied to the device once, so the
+ * prepared call below can run inside a captured CUDA graph. */
+int irs_dc_set_segments(irs_distance_comparator* dc, size_t n_slots, const uint32_t* seg_start,
+                        const uint32_t* seg_query, const uint32_t* seg_mask);
+/* irs_dc_compare_threshold_open with the stored segment table; performs no
+ * host synchronisation (graph-capturable). */
+int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circuits* c,
+                                           irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3],
+                                           size_t offset, size_t len, uint32_t threshold_a, int self_check,
+                                           void* stream);
 /* Match bitmap in the reference layout: bit (q * db_len + e) set if query q
  * matches entry e (u64 words, ceil(n_queries * db_len / 64)). */
 int irs_dc_fetch_bitmap(irs_distance_comparator* dc, size_t n_queries, size_t db_len, uint64_t* host);
@@ -270,6 +306,18 @@ int irs_dc_join_batch_matches(irs_distance_comparator* dc, irs_distance_comparat
  * 0xFFFFFFFE for an in-batch duplicate, 0xFFFFFFFF for no match. */
 int irs_dc_fetch_final_results(irs_distance_comparator* dc, size_t n_queries, uint32_t* final_results,
                                uint32_t* match_counters, uint32_t* all_matches);
+
+/* ------------------------------------------------------------------------ */
+/* CUDA graphs of a batch's device work (party 0's stream).                  */
+/* Between begin and end, the library keeps all launches on the capturing    */
+/* stream (no cross-party event waits); calls that synchronise the host fail */
+/* with the CUDA capture error.                                              */
+/* ------------------------------------------------------------------------ */
+typedef struct irs_graph irs_graph;
+int irs_graph_begin_capture(irs_device_manager* dm);
+int irs_graph_end_capture(irs_device_manager* dm, irs_graph** out);
+int irs_graph_launch(irs_graph* g, void* stream);
+int irs_graph_destroy(irs_graph* g);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,13 @@ struct irs_device_manager {
   cudaStream_t streams[3] = {nullptr, nullptr, nullptr};
   cudaMemPool_t pools[3] = {nullptr, nullptr, nullptr};
   int* d_err = nullptr;
+  uint64_t* d_batch = nullptr;  // device batch counter (irs_device_manager_set_batch_counter)
+  bool capturing = false;  // a graph capture on streams[0] is open
+};
+
+struct irs_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
 
 struct irs_sharedb {
@@ -76,7 +83,11 @@ struct irs_sharedb {
   uint8_t* q_hi = nullptr;
   uint16_t* q_stage = nullptr;  // u16 staging [n_pad][K]
   QuerySlot* d_slots = nullptr;
-  size_t n_pad = 0;
+  size_t n_pad = 0;          // active padded query rows (result row stride)
+  size_t n_cap = 0;          // query row capacity
+  size_t rows_uploaded = 0;  // rows of the last upload
+  int tile_override = 0;     // tile width requested by irs_sharedb_set_tile (0 = auto)
+  bool batch_from_device = false;
   bool have_query = false;
   // results [max_db][n_pad] u16 (entry-major)
   uint16_t* results = nullptr;
@@ -91,6 +102,7 @@ struct irs_circuits {
   irs_device_manager* dm = nullptr;
   ChaChaKey keys[3]{};
   uint64_t batch = 0;
+  bool batch_from_device = false;
 };
 
 struct irs_distance_comparator {
@@ -107,6 +119,12 @@ struct irs_distance_comparator {
   uint32_t* d_slot_valid = nullptr;
   uint32_t* d_slot_query = nullptr;
   size_t slot_cap = 0;
+  // segment table (irs_dc_set_segments)
+  uint32_t* d_seg_start = nullptr;  // [slot_cap + 1]
+  uint32_t* d_seg_query = nullptr;  // [seg_cap]
+  uint32_t* d_seg_mask = nullptr;   // [seg_cap]
+  size_t seg_cap = 0, n_seg_slots = 0;
+  bool have_segments = false;
 };
 
 namespace {
@@ -144,6 +162,30 @@ ChaChaKey key_of(const uint32_t k[8]) {
   ChaChaKey r;
   for (int i = 0; i < 8; i++) r.k[i] = k[i];
   return r;
+}
+
+// Query tensor maps for the current tile width (the two-SM GEMM loads half of
+// a query tile per CTA).
+int rebuild_query_maps(irs_sharedb* db) {
+  if (db->block_n <= 0) return IRS_OK;  // no valid tile width: dot reports it
+  const uint32_t q_box = (uint32_t)(gemm_use_pair(db->block_n) ? db->block_n / 2 : db->block_n);
+  if (make_tmap_u8(&db->tm_q_lo, db->q_lo, db->n_cap, db->code_length, q_box) ||
+      make_tmap_u8(&db->tm_q_hi, db->q_hi, db->n_cap, db->code_length, q_box))
+    return fail(IRS_ERR_CUDA, "tensor map for the query planes failed");
+  return IRS_OK;
+}
+
+// Sets the active padded row count and tile width for `rows` query rows.
+int set_active_rows(irs_sharedb* db, size_t rows) {
+  const size_t n = round_up(rows ? rows : 1, 64);
+  if (n > db->n_cap) return fail(IRS_ERR_INVALID, "%zu rows exceed the query capacity %zu", rows, db->n_cap);
+  int bn = gemm_block_n_for((uint32_t)n);
+  if (db->tile_override && n % (size_t)db->tile_override == 0) bn = db->tile_override;
+  const bool rebuild = bn != db->block_n;
+  db->n_pad = n;
+  db->block_n = bn;
+  db->rows_uploaded = rows;
+  return rebuild ? rebuild_query_maps(db) : IRS_OK;
 }
 
 }  // namespace
@@ -184,6 +226,8 @@ int irs_device_manager_init(int device, irs_device_manager** out) {
   }
   CU(cudaMalloc(&dm->d_err, sizeof(int)));
   CU(cudaMemset(dm->d_err, 0, sizeof(int)));
+  CU(cudaMalloc(&dm->d_batch, sizeof(uint64_t)));
+  CU(cudaMemset(dm->d_batch, 0, sizeof(uint64_t)));
   *out = dm;
   return IRS_OK;
 }
@@ -193,6 +237,7 @@ int irs_device_manager_destroy(irs_device_manager* dm) {
   cudaSetDevice(dm->device);
   for (int p = 0; p < 3; p++) if (dm->streams[p]) cudaStreamSynchronize(dm->streams[p]);
   cudaFree(dm->d_err);
+  cudaFree(dm->d_batch);
   for (int p = 0; p < 3; p++) {
     if (dm->streams[p]) cudaStreamDestroy(dm->streams[p]);
     if (dm->pools[p]) cudaMemPoolDestroy(dm->pools[p]);
@@ -222,6 +267,30 @@ int irs_device_manager_error(irs_device_manager* dm, int* code) {
 int irs_device_manager_clear_error(irs_device_manager* dm) {
   CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
   CU(cudaMemset(dm->d_err, 0, sizeof(int)));
+  return IRS_OK;
+}
+
+int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_id, void* stream) {
+  CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
+  CHECK(batch_id < (1ull << 24), IRS_ERR_INVALID, "batch id must be below 2^24");
+  CHECK(!dm->capturing, IRS_ERR_STATE, "set the batch counter outside a graph capture");
+  static thread_local uint64_t staged;  // pageable source; the copy is synchronised below
+  staged = batch_id;
+  cudaStream_t s = party_stream(dm, 0, stream);
+  CU(cudaMemcpyAsync(dm->d_batch, &staged, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  CU(cudaStreamSynchronize(s));
+  return IRS_OK;
+}
+
+int irs_sharedb_use_batch_counter(irs_sharedb* db, int on) {
+  CHECK(db, IRS_ERR_INVALID, "db is NULL");
+  db->batch_from_device = on != 0;
+  return IRS_OK;
+}
+
+int irs_circuits_use_batch_counter(irs_circuits* c, int on) {
+  CHECK(c, IRS_ERR_INVALID, "c is NULL");
+  c->batch_from_device = on != 0;
   return IRS_OK;
 }
 
@@ -302,7 +371,8 @@ int irs_sharedb_init(irs_device_manager* dm, int peer_id, size_t max_db_length, 
   db->seed0 = key_of(seed0);
   db->seed1 = key_of(seed1);
   db->remote = is_remote != 0;
-  db->n_pad = round_up(query_length, 64);
+  db->n_cap = round_up(query_length, 64);
+  db->n_pad = db->n_cap;
   db->block_n = gemm_block_n_for((uint32_t)db->n_pad);
   if (cudaEventCreateWithFlags(&db->done, cudaEventDisableTiming) != cudaSuccess) {
     delete db;
@@ -310,22 +380,19 @@ int irs_sharedb_init(irs_device_manager* dm, int peer_id, size_t max_db_length, 
   }
   int rc;
   void* p;
-  if ((rc = pool_alloc(dm, peer_id, db->n_pad * code_length, &p))) { irs_sharedb_destroy(db); return rc; }
+  if ((rc = pool_alloc(dm, peer_id, db->n_cap * code_length, &p))) { irs_sharedb_destroy(db); return rc; }
   db->q_lo = (uint8_t*)p;
-  if ((rc = pool_alloc(dm, peer_id, db->n_pad * code_length, &p))) { irs_sharedb_destroy(db); return rc; }
+  if ((rc = pool_alloc(dm, peer_id, db->n_cap * code_length, &p))) { irs_sharedb_destroy(db); return rc; }
   db->q_hi = (uint8_t*)p;
-  if ((rc = pool_alloc(dm, peer_id, db->n_pad * code_length * 2, &p))) { irs_sharedb_destroy(db); return rc; }
+  if ((rc = pool_alloc(dm, peer_id, db->n_cap * code_length * 2, &p))) { irs_sharedb_destroy(db); return rc; }
   db->q_stage = (uint16_t*)p;
-  if ((rc = pool_alloc(dm, peer_id, (db->n_pad / kSlotRows) * sizeof(QuerySlot), &p))) { irs_sharedb_destroy(db); return rc; }
+  if ((rc = pool_alloc(dm, peer_id, (db->n_cap / kSlotRows) * sizeof(QuerySlot), &p))) { irs_sharedb_destroy(db); return rc; }
   db->d_slots = (QuerySlot*)p;
-  if ((rc = pool_alloc(dm, peer_id, max_db_length * db->n_pad * 2, &p))) { irs_sharedb_destroy(db); return rc; }
+  if ((rc = pool_alloc(dm, peer_id, max_db_length * db->n_cap * 2, &p))) { irs_sharedb_destroy(db); return rc; }
   db->results = (uint16_t*)p;
-  // The two-SM GEMM loads half of a query tile per CTA.
-  const uint32_t q_box = (uint32_t)(gemm_use_pair(db->block_n) ? db->block_n / 2 : db->block_n);
-  if (make_tmap_u8(&db->tm_q_lo, db->q_lo, db->n_pad, code_length, q_box) ||
-      make_tmap_u8(&db->tm_q_hi, db->q_hi, db->n_pad, code_length, q_box)) {
+  if ((rc = rebuild_query_maps(db))) {
     irs_sharedb_destroy(db);
-    return fail(IRS_ERR_CUDA, "tensor map for the query planes failed");
+    return rc;
   }
   *out = db;
   return IRS_OK;
@@ -384,7 +451,7 @@ int irs_sharedb_load_records(irs_sharedb* db, size_t first, size_t n, const uint
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = dm->streams[db->peer];
   const size_t K = db->code_length;
-  const size_t per = std::max<size_t>(1, (db->n_pad * K) / K);  // reuse the query staging buffer
+  const size_t per = std::max<size_t>(1, db->n_cap);  // records per pass through the query staging buffer
   for (size_t done = 0; done < n;) {
     const size_t c = std::min(per, n - done);
     CU(cudaMemcpyAsync(db->q_stage, records + done * K, c * K * 2, cudaMemcpyHostToDevice, s));
@@ -393,7 +460,6 @@ int irs_sharedb_load_records(irs_sharedb* db, size_t first, size_t n, const uint
     done += c;
   }
   db->db_len = std::max(db->db_len, first + n);
-  db->have_query = false;  // staging reused
   return IRS_OK;
 }
 
@@ -476,7 +542,8 @@ int irs_sharedb_synth_db(irs_sharedb* const code_engines[3], irs_sharedb* const 
 
 int irs_sharedb_query_upload(irs_sharedb* db, const uint16_t* rows, size_t n_rows) {
   CHECK(db && (rows || !n_rows), IRS_ERR_INVALID, "bad arguments");
-  CHECK(n_rows <= db->n_pad, IRS_ERR_INVALID, "%zu rows exceed the padded query length %zu", n_rows, db->n_pad);
+  int rc = set_active_rows(db, n_rows);
+  if (rc) return rc;
   irs_device_manager* dm = db->dm;
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = dm->streams[db->peer];
@@ -491,15 +558,17 @@ int irs_sharedb_query_upload(irs_sharedb* db, const uint16_t* rows, size_t n_row
 int irs_sharedb_query_upload_slots(irs_sharedb* db, const uint16_t* base, size_t n_base, const irs_query_slot* slots,
                                    size_t n_slots) {
   CHECK(db && base && slots && n_base > 0, IRS_ERR_INVALID, "bad arguments");
-  CHECK(n_slots * kSlotRows <= db->n_pad, IRS_ERR_INVALID, "%zu slots exceed the padded query length %zu", n_slots,
-        db->n_pad);
-  CHECK(n_base <= db->n_pad, IRS_ERR_INVALID, "too many base queries");
+  CHECK(n_slots * kSlotRows <= db->n_cap, IRS_ERR_INVALID, "%zu slots exceed the query capacity %zu", n_slots,
+        db->n_cap);
+  CHECK(n_base <= db->n_cap, IRS_ERR_INVALID, "too many base queries");
   CHECK(db->code_length % kRowLen == 0, IRS_ERR_INVALID, "rotations need code_length a multiple of 800");
   for (size_t i = 0; i < n_slots; i++) {
     CHECK(slots[i].src < n_base && slots[i].n_rot <= (uint32_t)kRotations &&
               slots[i].rot_lo + slots[i].n_rot <= (uint32_t)kRotations,
           IRS_ERR_INVALID, "slot %zu is invalid", i);
   }
+  int rc = set_active_rows(db, n_slots * kSlotRows);
+  if (rc) return rc;
   irs_device_manager* dm = db->dm;
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = dm->streams[db->peer];
@@ -511,6 +580,64 @@ int irs_sharedb_query_upload_slots(irs_sharedb* db, const uint16_t* base, size_t
                          db->q_hi, s));
   CU(cudaStreamSynchronize(s));  // slots / base are caller-owned host memory
   db->have_query = true;
+  return IRS_OK;
+}
+
+int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t n_base, const uint32_t* row_desc,
+                                  size_t n_rows) {
+  CHECK(db && base && row_desc && n_base > 0, IRS_ERR_INVALID, "bad arguments");
+  CHECK(db->code_length % kRowLen == 0, IRS_ERR_INVALID, "rotations need code_length a multiple of 800");
+  const size_t K = db->code_length;
+  // staging: base queries, then the row table after them
+  const size_t base_bytes = n_base * K * 2, table_bytes = n_rows * 4;
+  CHECK(base_bytes + table_bytes + 16 <= db->n_cap * K * 2, IRS_ERR_INVALID, "too many base queries for the staging");
+  for (size_t r = 0; r < n_rows; r++)
+    CHECK(row_desc[r] == 0xFFFFFFFFu || ((row_desc[r] >> 8) < n_base && (row_desc[r] & 0xFFu) < (uint32_t)kRotations),
+          IRS_ERR_INVALID, "row %zu descriptor 0x%x is invalid", r, row_desc[r]);
+  int rc = set_active_rows(db, n_rows);
+  if (rc) return rc;
+  irs_device_manager* dm = db->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[db->peer];
+  uint8_t* stage = reinterpret_cast<uint8_t*>(db->q_stage);
+  const size_t table_off = (base_bytes + 15) / 16 * 16;
+  CU(cudaMemcpyAsync(stage, base, base_bytes, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(stage + table_off, row_desc, table_bytes, cudaMemcpyHostToDevice, s));
+  CU(launch_expand_rows(db->q_stage, (uint32_t)K, reinterpret_cast<const uint32_t*>(stage + table_off), (uint32_t)n_rows,
+                        (uint32_t)db->n_pad, db->q_lo, db->q_hi, s));
+  CU(cudaStreamSynchronize(s));  // base / row_desc are caller-owned host memory
+  db->have_query = true;
+  return IRS_OK;
+}
+
+int irs_sharedb_gather_records(irs_sharedb* dst, irs_sharedb* src, const uint32_t* ids, size_t n) {
+  CHECK(dst && src && (ids || !n), IRS_ERR_INVALID, "bad arguments");
+  CHECK(dst->dm == src->dm && dst->peer == src->peer && dst->code_length == src->code_length, IRS_ERR_INVALID,
+        "gather needs engines of the same party and code length");
+  CHECK(dst->db_lo && src->db_lo, IRS_ERR_STATE, "alloc_db not called");
+  CHECK(n <= dst->db_cap, IRS_ERR_INVALID, "%zu records exceed the destination capacity %zu", n, dst->db_cap);
+  for (size_t k = 0; k < n; k++)
+    CHECK(ids[k] < src->db_cap, IRS_ERR_INVALID, "record id %u out of range", ids[k]);
+  irs_device_manager* dm = dst->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[dst->peer];
+  const size_t K = dst->code_length;
+  CHECK(n * 4 <= dst->n_cap * K * 2, IRS_ERR_INVALID, "too many records for one gather");
+  // Staging reuse: the gather runs before the next query upload of `dst`.
+  CU(cudaMemcpyAsync(dst->q_stage, ids, n * 4, cudaMemcpyHostToDevice, s));
+  CU(launch_gather_rows(src->db_lo, src->db_hi, reinterpret_cast<const uint32_t*>(dst->q_stage), (uint32_t)n,
+                        (uint32_t)K, dst->db_lo, dst->db_hi, s));
+  CU(cudaStreamSynchronize(s));
+  dst->db_len = n;
+  return IRS_OK;
+}
+
+int irs_sharedb_set_tile(irs_sharedb* db, int block_n) {
+  CHECK(db, IRS_ERR_INVALID, "db is NULL");
+  CHECK(block_n == 0 || block_n == 64 || block_n == 128 || block_n == 256, IRS_ERR_INVALID,
+        "tile width %d is not 0, 64, 128 or 256", block_n);
+  db->tile_override = block_n;
+  if (db->have_query) return set_active_rows(db, db->rows_uploaded);
   return IRS_OK;
 }
 
@@ -545,6 +672,7 @@ static int fill_problem(irs_sharedb* db, uint16_t mult, size_t offset, size_t le
   pr.nonce = nonce_of(db->code_length == (size_t)kIrisCodeLength ? kDomCodeDot : kDomMaskDot,
                       (uint32_t)db->dm->device);
   pr.batch = db->batch;
+  pr.batch_dev = db->batch_from_device ? db->dm->d_batch : nullptr;
   return IRS_OK;
 }
 
@@ -564,9 +692,11 @@ int irs_sharedb_dot_many(irs_sharedb* const* engines, const uint16_t* multiplier
     if (rc) return rc;
   }
   cudaStream_t s = party_stream(dm, engines[0]->peer, stream);
-  // The engines' inputs may have been written on their own party streams.
+  // The engines' inputs may have been written on their own party streams
+  // (not while a graph is being captured: then all work is on the capture
+  // stream and the uploads happened before the capture began).
   for (int i = 0; i < n; i++)
-    if (dm->streams[engines[i]->peer] != s) {
+    if (!dm->capturing && dm->streams[engines[i]->peer] != s) {
       CU(cudaEventRecord(engines[i]->done, dm->streams[engines[i]->peer]));
       CU(cudaStreamWaitEvent(s, engines[i]->done, 0));
     }
@@ -598,7 +728,8 @@ int irs_sharedb_fetch_results(irs_sharedb* db, uint16_t* host, size_t len) {
   int rc = check_device_error(dm);
   if (rc) return rc;
   for (size_t m = 0; m < len; m++)
-    for (size_t q = 0; q < db->query_length; q++) host[q * len + m] = tmp[m * db->n_pad + q];
+    for (size_t q = 0; q < db->query_length; q++)
+      host[q * len + m] = q < db->n_pad ? tmp[m * db->n_pad + q] : (uint16_t)0;
   return IRS_OK;
 }
 
@@ -643,6 +774,7 @@ static void base_params(irs_circuits* c, ThresholdParams& P) {
   for (int p = 0; p < 3; p++) P.key[p] = c->keys[p];
   P.nonce = nonce_of(kDomCircuit, (uint32_t)c->dm->device);
   P.batch = c->batch;
+  P.batch_dev = c->batch_from_device ? c->dm->d_batch : nullptr;
 }
 
 // Splits [3][n/32] result components into each party's (a, b) u64 words.
@@ -762,6 +894,7 @@ int irs_dc_init(irs_device_manager* dm, size_t max_queries, size_t max_db_length
   dc->self_stride_bits = round_up(max_queries, 64);
   dc->match_cap = match_list_cap ? match_list_cap : 1;
   dc->slot_cap = 65536 / kSlotRows;
+  dc->seg_cap = dc->slot_cap * 32;
   struct { void** p; size_t bytes; } allocs[] = {
       {(void**)&dc->bitmap, max_queries * dc->stride_bits / 8},
       {(void**)&dc->self_bitmap, max_queries * dc->self_stride_bits / 8},
@@ -773,6 +906,9 @@ int irs_dc_init(irs_device_manager* dm, size_t max_queries, size_t max_db_length
       {(void**)&dc->all_matches, max_queries * kMaxMatchesLen * 4},
       {(void**)&dc->d_slot_valid, dc->slot_cap * 4},
       {(void**)&dc->d_slot_query, dc->slot_cap * 4},
+      {(void**)&dc->d_seg_start, (dc->slot_cap + 1) * 4},
+      {(void**)&dc->d_seg_query, dc->slot_cap * 32 * 4},
+      {(void**)&dc->d_seg_mask, dc->slot_cap * 32 * 4},
   };
   for (auto& a : allocs) {
     cudaError_t e = cudaMalloc(a.p, a.bytes);
@@ -793,7 +929,8 @@ int irs_dc_destroy(irs_distance_comparator* dc) {
   if (!dc) return IRS_OK;
   cudaSetDevice(dc->dm->device);
   void* ps[] = {dc->bitmap, dc->self_bitmap, dc->match_list, dc->counters, dc->partial, dc->final_results,
-                dc->match_counters, dc->all_matches, dc->d_slot_valid, dc->d_slot_query};
+                dc->match_counters, dc->all_matches, dc->d_slot_valid, dc->d_slot_query,
+                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask};
   for (void* p : ps) if (p) cudaFree(p);
   delete dc;
   return IRS_OK;
@@ -867,6 +1004,128 @@ int irs_dc_compare_threshold_open(irs_distance_comparator* dc, irs_circuits* c, 
   P.match_cap = (uint32_t)dc->match_cap;
   CU(launch_threshold_bitmap(P, s));
   if (slot_valid || slot_query) CU(cudaStreamSynchronize(s));  // host arrays are caller-owned
+  return IRS_OK;
+}
+
+int irs_dc_set_segments(irs_distance_comparator* dc, size_t n_slots, const uint32_t* seg_start,
+                        const uint32_t* seg_query, const uint32_t* seg_mask) {
+  CHECK(dc && seg_start && n_slots > 0 && n_slots <= dc->slot_cap, IRS_ERR_INVALID, "bad arguments");
+  CHECK(seg_start[0] == 0, IRS_ERR_INVALID, "seg_start[0] must be 0");
+  for (size_t i = 0; i < n_slots; i++)
+    CHECK(seg_start[i + 1] >= seg_start[i], IRS_ERR_INVALID, "seg_start must be non-decreasing");
+  const size_t n_seg = seg_start[n_slots];
+  CHECK(n_seg <= dc->seg_cap && (n_seg == 0 || (seg_query && seg_mask)), IRS_ERR_INVALID, "too many segments");
+  for (size_t k = 0; k < n_seg; k++)
+    CHECK(seg_query[k] < dc->max_queries, IRS_ERR_INVALID, "segment %zu reports to query %u >= max", k, seg_query[k]);
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[0];
+  CU(cudaMemcpyAsync(dc->d_seg_start, seg_start, (n_slots + 1) * 4, cudaMemcpyHostToDevice, s));
+  if (n_seg) {
+    CU(cudaMemcpyAsync(dc->d_seg_query, seg_query, n_seg * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(dc->d_seg_mask, seg_mask, n_seg * 4, cudaMemcpyHostToDevice, s));
+  }
+  CU(cudaStreamSynchronize(s));
+  dc->n_seg_slots = n_slots;
+  dc->have_segments = true;
+  return IRS_OK;
+}
+
+int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circuits* c,
+                                           irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3],
+                                           size_t offset, size_t len, uint32_t threshold_a, int self_check,
+                                           void* stream) {
+  CHECK(dc && c && code_engines && mask_engines, IRS_ERR_INVALID, "bad arguments");
+  CHECK(dc->have_segments, IRS_ERR_STATE, "irs_dc_set_segments not called");
+  CHECK(offset % 32 == 0, IRS_ERR_INVALID, "offset must be a multiple of 32");
+  const size_t n_pad = code_engines[0]->n_pad;
+  CHECK(dc->n_seg_slots * kSlotRows <= n_pad, IRS_ERR_INVALID, "segment slots exceed the padded query rows");
+  for (int p = 0; p < 3; p++) {
+    CHECK(code_engines[p] && mask_engines[p], IRS_ERR_INVALID, "engine missing");
+    CHECK(code_engines[p]->n_pad == n_pad && mask_engines[p]->n_pad == n_pad, IRS_ERR_INVALID,
+          "engines need the same query padding");
+    CHECK(code_engines[p]->res_offset == offset && mask_engines[p]->res_offset == offset &&
+              code_engines[p]->res_len >= len && mask_engines[p]->res_len >= len,
+          IRS_ERR_STATE, "engine results do not cover entries %zu..%zu", offset, offset + len);
+  }
+  const size_t stride_bits = self_check ? dc->self_stride_bits : dc->stride_bits;
+  CHECK(offset + len <= stride_bits, IRS_ERR_INVALID, "entries exceed the bitmap width");
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = party_stream(dm, 0, stream);
+  for (int p = 0; p < 3; p++) {
+    CU(cudaStreamWaitEvent(s, code_engines[p]->done, 0));
+    CU(cudaStreamWaitEvent(s, mask_engines[p]->done, 0));
+  }
+  ThresholdParams P;
+  base_params(c, P);
+  for (int p = 0; p < 3; p++) {
+    P.code[p] = code_engines[p]->results;
+    P.mask[p] = mask_engines[p]->results;
+  }
+  P.threshold_a = threshold_a;
+  P.n_entries = (uint32_t)len;
+  P.m0 = (uint32_t)offset;
+  P.n_pad = (uint32_t)n_pad;
+  P.n_slots = (uint32_t)dc->n_seg_slots;
+  P.seg_start = dc->d_seg_start;
+  P.seg_query = dc->d_seg_query;
+  P.seg_mask = dc->d_seg_mask;
+  P.bitmap = self_check ? dc->self_bitmap : dc->bitmap;
+  P.bitmap_stride = (uint32_t)stride_bits;
+  P.match_count = dc->counters;
+  P.match_list = self_check ? nullptr : dc->match_list;
+  P.match_cap = (uint32_t)dc->match_cap;
+  CU(launch_threshold_bitmap(P, s));
+  return IRS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA graphs
+// ---------------------------------------------------------------------------
+int irs_graph_begin_capture(irs_device_manager* dm) {
+  CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
+  CHECK(!dm->capturing, IRS_ERR_STATE, "a capture is already open");
+  CU(cudaSetDevice(dm->device));
+  CU(cudaStreamBeginCapture(dm->streams[0], cudaStreamCaptureModeThreadLocal));
+  dm->capturing = true;
+  return IRS_OK;
+}
+
+int irs_graph_end_capture(irs_device_manager* dm, irs_graph** out) {
+  CHECK(dm && out, IRS_ERR_INVALID, "bad arguments");
+  CHECK(dm->capturing, IRS_ERR_STATE, "no capture is open");
+  *out = nullptr;
+  dm->capturing = false;
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamEndCapture(dm->streams[0], &g));
+  auto* gr = new (std::nothrow) irs_graph();
+  if (!gr) {
+    cudaGraphDestroy(g);
+    return fail(IRS_ERR_NOMEM, "host allocation failed");
+  }
+  gr->graph = g;
+  cudaError_t e = cudaGraphInstantiate(&gr->exec, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    delete gr;
+    return fail(IRS_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  }
+  *out = gr;
+  return IRS_OK;
+}
+
+int irs_graph_launch(irs_graph* g, void* stream) {
+  CHECK(g && g->exec, IRS_ERR_INVALID, "graph is NULL");
+  CU(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+  return IRS_OK;
+}
+
+int irs_graph_destroy(irs_graph* g) {
+  if (!g) return IRS_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
   return IRS_OK;
 }
 
@@ -995,6 +1254,7 @@ int circuit_view(irs_circuits* c, CircuitView* v) {
   for (int p = 0; p < 3; p++) v->keys[p] = c->keys[p];
   v->nonce = nonce_of(kDomCircuit, (uint32_t)c->dm->device);
   v->batch = c->batch;
+  v->batch_dev = c->batch_from_device ? c->dm->d_batch : nullptr;
   v->device = c->dm->device;
   v->stream0 = c->dm->streams[0];
   return IRS_OK;

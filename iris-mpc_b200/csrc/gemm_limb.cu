@@ -329,8 +329,9 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
           }
           if (pr.mask_on) {
             const uint64_t blk = (m_global * pr.n_pad + n) >> 5;
+            const uint64_t batch = pr.batch_dev ? *pr.batch_dev : pr.batch;
             uint32_t ks[32];
-            chacha12_pair(&pr.key_own, &pr.key_prev, counter_of(pr.batch, blk), pr.nonce, ks);
+            chacha12_pair(&pr.key_own, &pr.key_prev, counter_of(batch, blk), pr.nonce, ks);
 #pragma unroll
             for (int j = 0; j < 16; j++) v[j] = sub2(add2(v[j], ks[j]), ks[16 + j]);
           }
@@ -612,8 +613,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           }
           if (pr.mask_on) {
             const uint64_t blk = (m_global * pr.n_pad + n) >> 5;
+            const uint64_t batch = pr.batch_dev ? *pr.batch_dev : pr.batch;
             uint32_t ks[32];
-            chacha12_pair(&pr.key_own, &pr.key_prev, counter_of(pr.batch, blk), pr.nonce, ks);
+            chacha12_pair(&pr.key_own, &pr.key_prev, counter_of(batch, blk), pr.nonce, ks);
 #pragma unroll
             for (int j = 0; j < 16; j++) v[j] = sub2(add2(v[j], ks[j]), ks[16 + j]);
           }

@@ -25,6 +25,7 @@ struct alignas(64) GemmProblem {
   ChaChaKey key_prev;
   uint64_t nonce;
   uint64_t batch;
+  const uint64_t* batch_dev;  // when set, the batch id is read from device memory
   uint32_t tiles_m;     // filled by launch_limb_gemm
   uint32_t tiles_n;
 };

@@ -203,6 +203,24 @@ int irs_preprocess_query_share(int party, uint16_t* coefs, size_t n) {
   return IRS_OK;
 }
 
+int irs_mirror_query_share(uint16_t* coefs, size_t n, int flip_imaginary) {
+  if (!coefs || (n != 12800 && n != 6400)) return IRS_ERR_INVALID;
+  u16 tmp[12800], out[12800];
+  memcpy(tmp, coefs, n * 2);
+  // The imaginary half (b = 1) is negated: the reference subtracts it from a
+  // sharing of zero; the all-zero sharing gives the same plaintext.
+  if (flip_imaginary)
+    for (size_t i = 6400; i < n; i++) tmp[i] = (u16)(0 - tmp[i]);
+  for (size_t i = 0; i < n; i++) {
+    const int b = (int)i / 6400, w = (int)i % 6400 / 3200, r1 = (int)i % 3200 / 800, c = (int)i % 800 / 4,
+              r2 = (int)i % 4;
+    const int fc = c < 100 ? 99 - c : 199 - (c - 100);
+    out[b * 6400 + w * 3200 + r1 * 800 + fc * 4 + r2] = tmp[i];
+  }
+  memcpy(coefs, out, n * 2);
+  return IRS_OK;
+}
+
 int irs_synth_queries(uint64_t db_seed, uint64_t q_seed, size_t n_queries, const int64_t* planted_entry,
                       const int32_t* planted_rot, int preprocess, uint16_t* code_out, uint16_t* mask_out) {
   if (!code_out || !mask_out) return IRS_ERR_INVALID;

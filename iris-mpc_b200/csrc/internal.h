@@ -12,6 +12,7 @@ struct CircuitView {
   ChaChaKey keys[3];
   uint64_t nonce;
   uint64_t batch;
+  const uint64_t* batch_dev;
   int device;
   cudaStream_t stream0;  // party 0's stream
 };

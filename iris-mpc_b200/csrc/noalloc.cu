@@ -110,6 +110,7 @@ extern "C" int irs_circuits_compare_threshold_masked_many_noalloc(irs_circuits* 
   }
   P.nonce = v.nonce;
   P.batch = v.batch;
+  P.batch_dev = v.batch_dev;
   P.threshold_a = threshold_a;
   P.n_words = n / 32;
   P.word_base = 0;

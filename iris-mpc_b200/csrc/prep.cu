@@ -65,6 +65,47 @@ __global__ void expand_slots_kernel(const uint16_t* __restrict__ base, uint32_t 
   reinterpret_cast<uint32_t*>(hi)[i] = h;
 }
 
+// One thread per (row, 4-coefficient block).  row_desc[r] = (src << 8) | rot
+// puts rotation `rot` (0..30, 15 = centre) of base query `src` in row r;
+// 0xFFFFFFFF leaves the row zero.  Lets a batch pack queries with different
+// rotation counts densely (no 32-row slot per query).
+__global__ void expand_rows_kernel(const uint16_t* __restrict__ base, uint32_t K, const uint32_t* __restrict__ row_desc,
+                                   uint32_t n_rows, uint32_t n_pad, uint8_t* __restrict__ lo, uint8_t* __restrict__ hi) {
+  const uint32_t blocks_per_row = K / 4;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)n_pad * blocks_per_row) return;
+  const uint32_t row = (uint32_t)(i / blocks_per_row);
+  const uint32_t b = (uint32_t)(i % blocks_per_row);
+  uint32_t l = 0, h = 0;
+  const uint32_t d = row < n_rows ? row_desc[row] : 0xFFFFFFFFu;
+  if (d != 0xFFFFFFFFu) {
+    const uint32_t src = d >> 8, rot = d & 0xFFu;
+    const int left_blocks = 15 - (int)rot;
+    const uint32_t row800 = b / 200, col = b % 200;
+    const uint32_t src_col = (uint32_t)(((int)col + left_blocks % 200 + 200) % 200);
+    const uint2 v = *reinterpret_cast<const uint2*>(base + (size_t)src * K + (size_t)row800 * kRowLen + (size_t)src_col * 4);
+    l = (v.x & 0xFFu) | ((v.x >> 8) & 0xFF00u) | ((v.y & 0xFFu) << 16) | ((v.y & 0xFF0000u) << 8);
+    h = ((v.x >> 8) & 0xFFu) | ((v.x >> 16) & 0xFF00u) | ((v.y & 0xFF00u) << 8) | (v.y & 0xFF000000u);
+  }
+  reinterpret_cast<uint32_t*>(lo)[i] = l;
+  reinterpret_cast<uint32_t*>(hi)[i] = h;
+}
+
+// Copies DB rows ids[k] of (src_lo, src_hi) into rows k of (dst_lo, dst_hi),
+// 16 bytes per thread (prefetch_subset, iris-mpc-gpu/src/dot/share_db.rs:344-407,
+// done device-to-device because the DB is resident).
+__global__ void gather_rows_kernel(const uint8_t* __restrict__ src_lo, const uint8_t* __restrict__ src_hi,
+                                   const uint32_t* __restrict__ ids, uint32_t n, uint32_t K, uint8_t* __restrict__ dst_lo,
+                                   uint8_t* __restrict__ dst_hi) {
+  const uint32_t per_row = K / 16;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)n * per_row) return;
+  const uint32_t k = (uint32_t)(i / per_row), c = (uint32_t)(i % per_row);
+  const size_t s = (size_t)ids[k] * K + (size_t)c * 16, d = (size_t)k * K + (size_t)c * 16;
+  *reinterpret_cast<uint4*>(dst_lo + d) = *reinterpret_cast<const uint4*>(src_lo + s);
+  *reinterpret_cast<uint4*>(dst_hi + d) = *reinterpret_cast<const uint4*>(src_hi + s);
+}
+
 // ---------------- synthetic share database ----------------
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -171,6 +212,22 @@ cudaError_t launch_expand_slots(const uint16_t* base, uint32_t K, const QuerySlo
   const size_t total = (size_t)n_pad * (K / 4);
   if (!total) return cudaSuccess;
   expand_slots_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(base, K, slots, n_slots, n_pad, lo, hi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_expand_rows(const uint16_t* base, uint32_t K, const uint32_t* row_desc, uint32_t n_rows,
+                               uint32_t n_pad, uint8_t* lo, uint8_t* hi, cudaStream_t stream) {
+  const size_t total = (size_t)n_pad * (K / 4);
+  if (!total) return cudaSuccess;
+  expand_rows_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(base, K, row_desc, n_rows, n_pad, lo, hi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const uint8_t* src_lo, const uint8_t* src_hi, const uint32_t* ids, uint32_t n,
+                               uint32_t K, uint8_t* dst_lo, uint8_t* dst_hi, cudaStream_t stream) {
+  const size_t total = (size_t)n * (K / 16);
+  if (!total) return cudaSuccess;
+  gather_rows_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(src_lo, src_hi, ids, n, K, dst_lo, dst_hi);
   return cudaGetLastError();
 }
 

@@ -25,6 +25,10 @@ cudaError_t launch_split_limbs(const uint16_t* in, uint8_t* lo, uint8_t* hi, siz
 cudaError_t launch_xor80(uint8_t* p, size_t n, cudaStream_t stream);
 cudaError_t launch_expand_slots(const uint16_t* base, uint32_t K, const QuerySlot* slots, uint32_t n_slots,
                                 uint32_t n_pad, uint8_t* lo, uint8_t* hi, cudaStream_t stream);
+cudaError_t launch_expand_rows(const uint16_t* base, uint32_t K, const uint32_t* row_desc, uint32_t n_rows,
+                               uint32_t n_pad, uint8_t* lo, uint8_t* hi, cudaStream_t stream);
+cudaError_t launch_gather_rows(const uint8_t* src_lo, const uint8_t* src_hi, const uint32_t* ids, uint32_t n,
+                               uint32_t K, uint8_t* dst_lo, uint8_t* dst_hi, cudaStream_t stream);
 cudaError_t launch_synth_db(uint64_t seed, uint32_t first, uint32_t count, const SynthOut& out, cudaStream_t stream);
 
 }  // namespace irs

@@ -34,7 +34,7 @@ __device__ __forceinline__ void init_rand(WordRand& wr, const ThresholdParams& P
 #pragma unroll
   for (int s = 0; s < 3; s++) wr.key[s] = P.key[s];
   wr.nonce = P.nonce;
-  wr.base = counter_of(P.batch, word_id * (uint64_t)kCircuitBlocksPerWord);
+  wr.base = counter_of(P.batch_dev ? *P.batch_dev : P.batch, word_id * (uint64_t)kCircuitBlocksPerWord);
 }
 
 template <int STAGE>
@@ -76,26 +76,37 @@ __global__ void __launch_bounds__(kThreshThreads, MIN_BLOCKS) threshold_bitmap_k
   const uint16_t* mask[3] = {P.mask[0] + off, P.mask[1] + off, P.mask[2] + off};
   Comp msb;
   const uint32_t opened = threshold_word<kStageFull>(code, mask, P.threshold_a, wr, msb);
-  const uint32_t row_mask = P.slot_valid ? P.slot_valid[slot] : 0x7FFFFFFFu;
-  const bool match = valid && (opened & row_mask) != 0;
-  const uint32_t bits = __ballot_sync(0xFFFFFFFFu, match);
-  if (P.bitmap && lane == 0) {
-    const uint32_t query = P.slot_query ? P.slot_query[slot] : slot;
-    P.bitmap[(size_t)query * (P.bitmap_stride / 32) + (uint32_t)((P.m0 + group * 32) / 32)] = bits;
-  }
-  if (P.match_list && bits) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(P.match_count, (uint32_t)__popc(bits));
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (match) {
-      const uint32_t rank = (uint32_t)__popc(bits & ((1u << lane) - 1u));
-      const uint32_t pos = base + rank;
-      if (pos < P.match_cap) {
-        const uint32_t query = P.slot_query ? P.slot_query[slot] : slot;
-        P.match_list[2 * pos] = query;
-        P.match_list[2 * pos + 1] = (uint32_t)m_global;
+  const size_t bitmap_word = (size_t)((P.m0 + group * 32) / 32);
+  // Rotation OR of one query's rows, one ballot for the warp's 32 entries.
+  auto emit = [&](uint32_t query, uint32_t row_mask, bool shared_word) {
+    const bool match = valid && (opened & row_mask) != 0;
+    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, match);
+    if (P.bitmap && lane == 0) {
+      uint32_t* w = P.bitmap + (size_t)query * (P.bitmap_stride / 32) + bitmap_word;
+      if (shared_word) {
+        if (bits) atomicOr(w, bits);
+      } else {
+        *w = bits;
       }
     }
+    if (P.match_list && bits) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(P.match_count, (uint32_t)__popc(bits));
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (match) {
+        const uint32_t pos = base + (uint32_t)__popc(bits & ((1u << lane) - 1u));
+        if (pos < P.match_cap) {
+          P.match_list[2 * pos] = query;
+          P.match_list[2 * pos + 1] = (uint32_t)m_global;
+        }
+      }
+    }
+  };
+  if (P.seg_start) {
+    const uint32_t s0 = P.seg_start[slot], s1 = P.seg_start[slot + 1];
+    for (uint32_t k = s0; k < s1; k++) emit(P.seg_query[k], P.seg_mask[k], true);
+  } else {
+    emit(P.slot_query ? P.slot_query[slot] : slot, P.slot_valid ? P.slot_valid[slot] : 0x7FFFFFFFu, false);
   }
 }
 

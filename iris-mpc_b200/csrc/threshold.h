@@ -12,6 +12,7 @@ struct ThresholdParams {
   ChaChaKey key[3];         // stream p = party p's own seed
   uint64_t nonce;
   uint64_t batch;
+  const uint64_t* batch_dev;  // when set, the batch id is read from device memory
   uint32_t threshold_a;
   // flat mode
   uint64_t n_words;
@@ -25,6 +26,12 @@ struct ThresholdParams {
   uint32_t n_slots;     // 32-row query slots evaluated
   const uint32_t* slot_valid;  // [n_slots] valid-row mask, NULL = rows 0..30
   const uint32_t* slot_query;  // [n_slots] query index owning the slot, NULL = identity
+  // Optional segment table (several queries per 32-row slot): segments
+  // seg_start[s] .. seg_start[s+1]-1 of slot s report rows seg_mask[k] to
+  // query seg_query[k].  Overrides slot_valid / slot_query when set.
+  const uint32_t* seg_start;
+  const uint32_t* seg_query;
+  const uint32_t* seg_mask;
   uint32_t* bitmap;     // [queries][bitmap_stride/32], optional
   uint32_t bitmap_stride;      // bits per bitmap row (multiple of 32)
   uint32_t* match_count;

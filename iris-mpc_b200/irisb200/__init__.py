@@ -78,6 +78,19 @@ _SIGS = {
     "irs_sharedb_query_upload": [_vp, _vp, _sz],
     "irs_sharedb_query_upload_slots": [_vp, _vp, _sz, _vp, _sz],
     "irs_sharedb_set_batch": [_vp, _u64],
+    "irs_sharedb_set_tile": [_vp, _i],
+    "irs_sharedb_use_batch_counter": [_vp, _i],
+    "irs_circuits_use_batch_counter": [_vp, _i],
+    "irs_device_manager_set_batch_counter": [_vp, _u64, _vp],
+    "irs_sharedb_query_upload_rows": [_vp, _vp, _sz, _vp, _sz],
+    "irs_sharedb_gather_records": [_vp, _vp, _vp, _sz],
+    "irs_mirror_query_share": [_vp, _sz, _i],
+    "irs_dc_set_segments": [_vp, _sz, _vp, _vp, _vp],
+    "irs_dc_compare_threshold_open_prepared": [_vp, _vp, _vp, _vp, _sz, _sz, _u32, _i, _vp],
+    "irs_graph_begin_capture": [_vp],
+    "irs_graph_end_capture": [_vp, C.POINTER(_vp)],
+    "irs_graph_launch": [_vp, _vp],
+    "irs_graph_destroy": [_vp],
     "irs_sharedb_dot": [_vp, _sz, _sz, C.c_uint16, _vp],
     "irs_sharedb_dot_many": [_vp, _vp, _i, _sz, _sz, _vp],
     "irs_sharedb_fetch_results": [_vp, _vp, _sz],
@@ -211,6 +224,39 @@ def preprocess_query_share(party: int, coefs: np.ndarray) -> np.ndarray:
     return out
 
 
+def mirror_query_share(coefs: np.ndarray, flip_imaginary: bool) -> np.ndarray:
+    """mirrored_code (flip_imaginary) / mirrored_mask of a query share."""
+    out = np.ascontiguousarray(coefs, np.uint16).copy()
+    _check(lib().irs_mirror_query_share(_ptr(out), out.size, int(flip_imaginary)))
+    return out
+
+
+class Graph:
+    """A captured CUDA graph of device work issued on party 0's stream."""
+
+    def __init__(self, h):
+        self.h = h
+
+    @staticmethod
+    def capture(dm: "DeviceManager", fn) -> "Graph":
+        _check(lib().irs_graph_begin_capture(dm.h))
+        try:
+            fn()
+        finally:
+            g = _vp()
+            rc = lib().irs_graph_end_capture(dm.h, C.byref(g))
+        _check(rc)
+        return Graph(g.value)
+
+    def launch(self, stream=None) -> None:
+        _check(lib().irs_graph_launch(self.h, stream))
+
+    def close(self) -> None:
+        if self.h:
+            lib().irs_graph_destroy(self.h)
+            self.h = None
+
+
 def synth_queries(db_seed: int, q_seed: int, n_queries: int, planted: dict, preprocess: bool = True,
                   code_out: np.ndarray = None, mask_out: np.ndarray = None):
     """Seeded synthetic query shares; planted = {query: (db entry, rotation)}.
@@ -251,6 +297,9 @@ class DeviceManager:
         c = C.c_int()
         _check(lib().irs_device_manager_error(self.h, C.byref(c)))
         return c.value
+
+    def set_batch_counter(self, batch_id: int, stream=None) -> None:
+        _check(lib().irs_device_manager_set_batch_counter(self.h, batch_id, stream))
 
     def sm_count(self) -> int:
         c = C.c_int()
@@ -315,6 +364,23 @@ class ShareDB:
     def set_batch(self, batch_id: int) -> None:
         _check(lib().irs_sharedb_set_batch(self.h, batch_id))
 
+    def set_tile(self, block_n: int) -> None:
+        _check(lib().irs_sharedb_set_tile(self.h, block_n))
+
+    def use_batch_counter(self, on: bool = True) -> None:
+        _check(lib().irs_sharedb_use_batch_counter(self.h, int(on)))
+
+    def query_upload_rows(self, base: np.ndarray, row_desc) -> None:
+        """Rows row_desc[r] = (src << 8) | rotation, 0xFFFFFFFF = empty."""
+        b = np.ascontiguousarray(base, np.uint16).reshape(-1, self.code_length)
+        rd = np.ascontiguousarray(row_desc, np.uint32)
+        _check(lib().irs_sharedb_query_upload_rows(self.h, _ptr(b), b.shape[0], _ptr(rd), rd.size))
+
+    def gather_records(self, src: "ShareDB", ids) -> None:
+        """prefetch_subset: records ids[k] of src become records k of this engine."""
+        i = np.ascontiguousarray(ids, np.uint32)
+        _check(lib().irs_sharedb_gather_records(self.h, src.h, _ptr(i), i.size))
+
     def dot(self, offset: int, length: int, multiplier: int = 1, stream=None) -> None:
         """dot + dot_reduce_and_multiply (share_db.rs:800-905), fused."""
         _check(lib().irs_sharedb_dot(self.h, offset, length, multiplier, stream))
@@ -367,6 +433,9 @@ class Circuits:
     def set_batch(self, batch_id: int) -> None:
         _check(lib().irs_circuits_set_batch(self.h, batch_id))
 
+    def use_batch_counter(self, on: bool = True) -> None:
+        _check(lib().irs_circuits_use_batch_counter(self.h, int(on)))
+
     def compare_threshold_masked_many(self, code_a, mask_a, n: int, threshold_a: int, res_a=None, res_b=None,
                                       opened=None, stream=None) -> None:
         _check(lib().irs_circuits_compare_threshold_masked_many(
@@ -412,6 +481,21 @@ class DistanceComparator:
             self.h, circuits.h, C.cast(hc, _vp), C.cast(hm, _vp), offset, length, n_slots,
             _ptr(sv) if sv is not None else None, _ptr(sq) if sq is not None else None, threshold_a,
             int(self_check), stream))
+
+    def set_segments(self, seg_start, seg_query, seg_mask) -> None:
+        st = np.ascontiguousarray(seg_start, np.uint32)
+        sq = np.ascontiguousarray(seg_query, np.uint32)
+        sm = np.ascontiguousarray(seg_mask, np.uint32)
+        _check(lib().irs_dc_set_segments(self.h, st.size - 1, _ptr(st), _ptr(sq) if sq.size else None,
+                                         _ptr(sm) if sm.size else None))
+
+    def compare_threshold_open_prepared(self, circuits: Circuits, code_engines, mask_engines, offset: int,
+                                        length: int, threshold_a: int, self_check: bool = False,
+                                        stream=None) -> None:
+        hc = (_vp * 3)(*[e.h for e in code_engines])
+        hm = (_vp * 3)(*[e.h for e in mask_engines])
+        _check(lib().irs_dc_compare_threshold_open_prepared(self.h, circuits.h, C.cast(hc, _vp), C.cast(hm, _vp),
+                                                            offset, length, threshold_a, int(self_check), stream))
 
     def fetch_bitmap(self, n_queries: int, db_len: int) -> np.ndarray:
         """Reference layout: bit (q * db_len + e), u64 words."""

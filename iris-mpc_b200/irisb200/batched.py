@@ -1,0 +1,274 @@
+"""Batched launches of uneven requests on the resident share DB.
+
+A batch mixes uniqueness requests (the query against the whole DB) and reauth
+requests (the query against one target entry, iris-mpc-gpu/src/server/
+actor.rs:1465-1475), each with 1..31 centred rotations
+(IrisRotation::centered, iris-mpc-common/src/galois_engine.rs:651-653) and
+optionally a mirrored variant (galois_engine.rs:218-225,520-543;
+server/mod.rs:156-176).  Instead of one 32-row slot per query iris (the plain
+drop-in), the rows of all variants are packed densely into 32-row words: a
+word may carry several queries, each a contiguous run of rows, and the
+threshold kernel ORs each run separately (segment table).  Reauth variants
+run on a gathered subset (the target records copied device-to-device,
+prefetch_subset share_db.rs:344-407) instead of the whole DB.
+
+The device work of a batch -- comparator reset, the six limb GEMMs and the
+fused threshold/open/OR per DB chunk, the result merge -- is captured once per
+layout into a CUDA graph and replayed; the ChaCha batch id comes from the
+device batch counter, so a replay draws fresh randomness.  The autotuner picks
+the tile width along the query rows and the DB chunk length per padded row
+count by timing the candidates once.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (IRIS_CODE_LENGTH, MASK_CODE_LENGTH, MAX_MATCHES_LEN, Circuits, DeviceManager, DistanceComparator,
+               Graph, ShareDB, dot_many, mirror_query_share)
+
+MULTS = [1, 1, 1, 2, 2, 2]
+
+
+def centred_rotations(n_rot: int) -> range:
+    """Indices into all_rotations() of the n centred rotations (15 = centre)."""
+    if not 1 <= n_rot <= 31:
+        raise ValueError("1..31 rotations")
+    lo = (31 - n_rot) // 2
+    return range(lo, lo + n_rot)
+
+
+@dataclass
+class Request:
+    """One query iris of a batch.  code/mask: the three parties' preprocessed
+    query shares, [3][12800] and [3][6400] u16."""
+    code: np.ndarray
+    mask: np.ndarray
+    n_rot: int = 31
+    mirrored: bool = False
+    kind: str = "uniqueness"  # or "reauth"
+    target: int = -1
+
+
+@dataclass
+class Result:
+    matches: list = field(default_factory=list)         # matched entries (uniqueness, normal orientation)
+    mirror_matches: list = field(default_factory=list)  # matched entries of the mirrored variant
+    reauth_match: bool | None = None
+    reauth_mirror_match: bool | None = None
+
+
+@dataclass
+class Layout:
+    """Dense packing of the variants' rows into 32-row words."""
+    row_desc: np.ndarray   # [rows] (src << 8) | rotation, 0xFFFFFFFF = empty
+    seg_start: np.ndarray  # [n_slots + 1]
+    seg_query: np.ndarray  # [n_seg] variant index (bitmap row)
+    seg_mask: np.ndarray   # [n_seg] rows of the slot belonging to the variant
+    n_rows: int
+    n_slots: int
+
+
+def pack(variant_rows: list) -> Layout:
+    """First-fit decreasing packing of variants (each a list of rotation
+    indices, reported as bitmap row = its index) into 32-row words without
+    splitting a variant across words."""
+    order = sorted(range(len(variant_rows)), key=lambda v: -len(variant_rows[v]))
+    slots = []  # each: list of (variant, first row, n)
+    fill = []
+    for v in order:
+        n = len(variant_rows[v])
+        for s, used in enumerate(fill):
+            if used + n <= 32:
+                slots[s].append((v, used, n))
+                fill[s] += n
+                break
+        else:
+            slots.append([(v, 0, n)])
+            fill.append(n)
+    n_slots = len(slots)
+    row_desc = np.full(n_slots * 32, 0xFFFFFFFF, np.uint32)
+    seg_start = [0]
+    seg_query, seg_mask = [], []
+    for s, segs in enumerate(slots):
+        for v, first, n in segs:
+            for k, rot in enumerate(variant_rows[v]):
+                row_desc[s * 32 + first + k] = (v << 8) | rot
+            seg_query.append(v)
+            seg_mask.append(((1 << n) - 1) << first if n < 32 else 0xFFFFFFFF)
+        seg_start.append(len(seg_query))
+    return Layout(row_desc, np.array(seg_start, np.uint32), np.array(seg_query, np.uint32),
+                  np.array(seg_mask, np.uint32), n_slots * 32, n_slots)
+
+
+class BatchedEngine:
+    """Runs batches of Requests against the six resident engines (party p code
+    at code_engines[p], mask at mask_engines[p])."""
+
+    def __init__(self, dm: DeviceManager, code_engines, mask_engines, circuits: Circuits, max_variants: int = 512,
+                 max_reauth: int = 512, threshold_a: int = 16384, seeds=None, autotune: bool = True):
+        self.dm = dm
+        self.ce, self.me = list(code_engines), list(mask_engines)
+        self.c = circuits
+        self.threshold_a = threshold_a
+        self.max_variants = max_variants
+        self.db_len = self.ce[0].db_len()
+        self.dc = DistanceComparator(dm, max_variants, max(self.ce[0].db_len(), 64), match_list_cap=1 << 20)
+        # reauth subset: one record per reauth variant
+        self.max_reauth = max_reauth
+        seeds = seeds or [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
+        rows_cap = max_reauth * 2 * 32
+        self.sce = [ShareDB(p, dm, max_reauth, rows_cap, IRIS_CODE_LENGTH, seeds[p]) for p in range(3)]
+        self.sme = [ShareDB(p, dm, max_reauth, rows_cap, MASK_CODE_LENGTH, seeds[p]) for p in range(3)]
+        for e in self.sce + self.sme:
+            e.alloc_db(max_reauth)
+        self.sdc = DistanceComparator(dm, max_reauth, max_reauth, match_list_cap=1 << 16)
+        for e in self.ce + self.me + self.sce + self.sme:
+            e.use_batch_counter(True)
+        circuits.use_batch_counter(True)
+        self.batch_id = 1
+        self.graphs = {}
+        self.tuned = {}
+        self.autotune = autotune
+
+    # -- configuration -----------------------------------------------------
+    def _chunks(self, n: int, chunk: int):
+        out, off = [], 0
+        while off < n:
+            ln = min(chunk, n - off)
+            out.append((off, ln))
+            off += ln
+        return out
+
+    def _capture(self, n_slots: int, chunk: int) -> Graph:
+        engines = self.ce + self.me
+
+        def body():
+            self.dc.reset()
+            for off, ln in self._chunks(self.db_len, chunk):
+                dot_many(engines, MULTS, off, ln)
+                self.dc.compare_threshold_open_prepared(self.c, self.ce, self.me, off, ln, self.threshold_a)
+            self.dc.join_db_matches(self.max_variants, self.db_len)
+        return Graph.capture(self.dm, body)
+
+    def _tile_candidates(self, n_rows: int):
+        n_pad = (n_rows + 63) // 64 * 64
+        return [b for b in (256, 128, 64) if n_pad % b == 0]
+
+    def _chunk_candidates(self):
+        full = (self.db_len + 31) // 32 * 32
+        return sorted({full, min(full, 131072)}, reverse=True)
+
+    def _run_db_pass(self, layout: Layout, tile: int, chunk: int) -> None:
+        key = (layout.n_slots, tile, chunk, self.db_len)
+        for e in self.ce + self.me:
+            e.set_tile(tile)
+        g = self.graphs.get(key)
+        if g is None:
+            g = self._capture(layout.n_slots, chunk)
+            self.graphs[key] = g
+        self.dm.set_batch_counter(self.batch_id)
+        g.launch(self.dm.stream(0))
+
+    def _tune(self, layout: Layout):
+        n_pad = (layout.n_rows + 63) // 64 * 64
+        if n_pad in self.tuned:
+            return self.tuned[n_pad]
+        cands = [(t, ch) for t in self._tile_candidates(layout.n_rows) for ch in self._chunk_candidates()]
+        if not self.autotune or len(cands) == 1:
+            self.tuned[n_pad] = cands[0]
+            return cands[0]
+        best, best_t = None, float("inf")
+        for t, ch in cands:
+            self._run_db_pass(layout, t, ch)  # warm (and capture)
+            self.dm.synchronize()
+            t0 = time.perf_counter()
+            self._run_db_pass(layout, t, ch)
+            self.dm.synchronize()
+            el = time.perf_counter() - t0
+            if el < best_t:
+                best, best_t = (t, ch), el
+        self.tuned[n_pad] = best
+        return best
+
+    # -- one batch -----------------------------------------------------------
+    def run(self, requests: list) -> list:
+        uniq, reauth = [], []  # (request index, mirrored?)
+        for i, r in enumerate(requests):
+            dst = reauth if r.kind == "reauth" else uniq
+            dst.append((i, False))
+            if r.mirrored:
+                dst.append((i, True))
+        if len(uniq) > self.max_variants or len(reauth) > self.max_reauth:
+            raise ValueError("batch exceeds the engine's variant capacity")
+        results = [Result() for _ in requests]
+        if uniq:
+            self._run_uniqueness(requests, uniq, results)
+        if reauth:
+            self._run_reauth(requests, reauth, results)
+        self.batch_id = (self.batch_id + 1) % (1 << 24) or 1
+        return results
+
+    def _base(self, requests, variants):
+        code = np.zeros((3, len(variants), IRIS_CODE_LENGTH), np.uint16)
+        mask = np.zeros((3, len(variants), MASK_CODE_LENGTH), np.uint16)
+        for v, (i, mir) in enumerate(variants):
+            r = requests[i]
+            for p in range(3):
+                code[p, v] = mirror_query_share(r.code[p], True) if mir else r.code[p]
+                mask[p, v] = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
+        return code, mask
+
+    def _run_uniqueness(self, requests, variants, results):
+        layout = pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants])
+        code, mask = self._base(requests, variants)
+        for p in range(3):
+            self.ce[p].query_upload_rows(code[p], layout.row_desc)
+            self.me[p].query_upload_rows(mask[p], layout.row_desc)
+        self.dc.set_segments(layout.seg_start, layout.seg_query, layout.seg_mask)
+        tile, chunk = self._tune(layout)
+        self._run_db_pass(layout, tile, chunk)
+        final, counters, allm = self.dc.fetch_final_results(len(variants))
+        for v, (i, mir) in enumerate(variants):
+            ids = sorted(allm[v, :min(int(counters[v]), MAX_MATCHES_LEN)].tolist())
+            if mir:
+                results[i].mirror_matches = ids
+            else:
+                results[i].matches = ids
+
+    def _run_reauth(self, requests, variants, results):
+        ids = np.array([requests[i].target for i, _ in variants], np.uint32)
+        for p in range(3):
+            self.sce[p].gather_records(self.ce[p], ids)
+            self.sme[p].gather_records(self.me[p], ids)
+        layout = pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants])
+        code, mask = self._base(requests, variants)
+        for p in range(3):
+            self.sce[p].query_upload_rows(code[p], layout.row_desc)
+            self.sme[p].query_upload_rows(mask[p], layout.row_desc)
+        for e in self.sce + self.sme:
+            e.set_tile(0)
+        n = len(variants)
+        self.dm.set_batch_counter(self.batch_id)
+        self.sdc.reset()
+        self.sdc.set_segments(layout.seg_start, layout.seg_query, layout.seg_mask)
+        dot_many(self.sce + self.sme, MULTS, 0, n)
+        self.sdc.compare_threshold_open_prepared(self.c, self.sce, self.sme, 0, n, self.threshold_a)
+        self.dm.synchronize()
+        from . import bitmap_get
+        bm = bitmap_get(self.sdc.fetch_bitmap(n, n), n, n)
+        for v, (i, mir) in enumerate(variants):
+            hit = bool(bm[v, v])  # variant v against its own target (subset record v)
+            if mir:
+                results[i].reauth_mirror_match = hit
+            else:
+                results[i].reauth_match = hit
+
+    def close(self) -> None:
+        for g in self.graphs.values():
+            g.close()
+        self.graphs.clear()
+        for o in self.sce + self.sme + [self.dc, self.sdc]:
+            o.close()
