@@ -70,8 +70,14 @@ int irs_device_manager_clear_error(irs_device_manager* dm);
  * ChaCha batch id from device memory at run time, so a captured graph can be
  * replayed for every batch with a fresh counter (set here, outside capture). */
 int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_id, void* stream);
+/* Advances the device batch counter on the stream (b -> b mod (2^24 - 1) + 1)
+ * without a host round trip: a serving loop that launches one DB chunk per
+ * step draws fresh randomness for every step while the host runs ahead. */
+int irs_device_manager_advance_batch_counter(irs_device_manager* dm, void* stream);
 /* Number of SMs the persistent kernels size their grids to. */
 int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
+/* Free and total device memory (cudaMemGetInfo), for admission by free HBM. */
+int irs_device_manager_mem_info(irs_device_manager* dm, size_t* free_bytes, size_t* total_bytes);
 
 /* Plain device memory helpers for callers that stage their own buffers. */
 int irs_device_alloc(irs_device_manager* dm, size_t bytes, void** ptr);
@@ -161,6 +167,14 @@ int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t 
 /* prefetch_subset (share_db.rs:344-407), device to device: copies DB records
  * ids[k] of `src` into records k of `dst` (same party and code length) and
  * sets dst's length to n.  Used for reauth targets and subset re-checks. */
+/* Resident base-query pool for a serving loop: writes preprocessed base
+ * queries [first, first + n) of the pool (the query staging area) without
+ * touching the others, so a request admitted while others are in flight costs
+ * one upload of its own shares. */
+int irs_sharedb_query_put_base(irs_sharedb* db, size_t first, size_t n, const uint16_t* base);
+/* irs_sharedb_query_upload_rows over the resident pool [0, n_base): rebuilds
+ * the query rows from the row table alone. */
+int irs_sharedb_query_expand_rows(irs_sharedb* db, size_t n_base, const uint32_t* row_desc, size_t n_rows);
 int irs_sharedb_gather_records(irs_sharedb* dst, irs_sharedb* src, const uint32_t* ids, size_t n);
 /* mirrored_code / mirrored_mask (galois_engine.rs:218-225,520-543) of a
  * (preprocessed or raw) query share, in place; flip_imaginary = 1 for codes. */
@@ -282,6 +296,14 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
                                            irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3],
                                            size_t offset, size_t len, uint32_t threshold_a, int self_check,
                                            void* stream);
+/* Clears bitmap rows [first, first + n) (a query row reused by the serving
+ * loop for a new request). */
+int irs_dc_clear_rows(irs_distance_comparator* dc, size_t first, size_t n, void* stream);
+/* Bitmap rows [first, first + n) in the internal layout: u32 words
+ * [n][row_words], bit j of word w = entry 32w + j; *row_words receives the
+ * words per row (the bitmap stride). */
+int irs_dc_fetch_rows(irs_distance_comparator* dc, size_t first, size_t n, uint32_t* host, size_t cap_words,
+                      size_t* row_words);
 /* Match bitmap in the reference layout: bit (q * db_len + e) set if query q
  * matches entry e (u64 words, ceil(n_queries * db_len / 64)). */
 int irs_dc_fetch_bitmap(irs_distance_comparator* dc, size_t n_queries, size_t db_len, uint64_t* host);

@@ -61,9 +61,11 @@ struct irs_device_manager {
   int* d_err = nullptr;
   uint64_t* d_batch = nullptr;  // device batch counter (irs_device_manager_set_batch_counter)
   bool capturing = false;  // a graph capture on streams[0] is open
+  cudaEvent_t graph_done = nullptr;  // recorded after each graph launch
 };
 
 struct irs_graph {
+  irs_device_manager* dm = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -228,6 +230,7 @@ int irs_device_manager_init(int device, irs_device_manager** out) {
   CU(cudaMemset(dm->d_err, 0, sizeof(int)));
   CU(cudaMalloc(&dm->d_batch, sizeof(uint64_t)));
   CU(cudaMemset(dm->d_batch, 0, sizeof(uint64_t)));
+  CU(cudaEventCreateWithFlags(&dm->graph_done, cudaEventDisableTiming));
   *out = dm;
   return IRS_OK;
 }
@@ -238,6 +241,7 @@ int irs_device_manager_destroy(irs_device_manager* dm) {
   for (int p = 0; p < 3; p++) if (dm->streams[p]) cudaStreamSynchronize(dm->streams[p]);
   cudaFree(dm->d_err);
   cudaFree(dm->d_batch);
+  if (dm->graph_done) cudaEventDestroy(dm->graph_done);
   for (int p = 0; p < 3; p++) {
     if (dm->streams[p]) cudaStreamDestroy(dm->streams[p]);
     if (dm->pools[p]) cudaMemPoolDestroy(dm->pools[p]);
@@ -282,6 +286,16 @@ int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_
   return IRS_OK;
 }
 
+__global__ void advance_batch_counter_kernel(uint64_t* b) { *b = *b % ((1ull << 24) - 1) + 1; }
+
+int irs_device_manager_advance_batch_counter(irs_device_manager* dm, void* stream) {
+  CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
+  CU(cudaSetDevice(dm->device));
+  advance_batch_counter_kernel<<<1, 1, 0, party_stream(dm, 0, stream)>>>(dm->d_batch);
+  CU(cudaGetLastError());
+  return IRS_OK;
+}
+
 int irs_sharedb_use_batch_counter(irs_sharedb* db, int on) {
   CHECK(db, IRS_ERR_INVALID, "db is NULL");
   db->batch_from_device = on != 0;
@@ -291,6 +305,13 @@ int irs_sharedb_use_batch_counter(irs_sharedb* db, int on) {
 int irs_circuits_use_batch_counter(irs_circuits* c, int on) {
   CHECK(c, IRS_ERR_INVALID, "c is NULL");
   c->batch_from_device = on != 0;
+  return IRS_OK;
+}
+
+int irs_device_manager_mem_info(irs_device_manager* dm, size_t* free_bytes, size_t* total_bytes) {
+  CHECK(dm && free_bytes && total_bytes, IRS_ERR_INVALID, "bad arguments");
+  CU(cudaSetDevice(dm->device));
+  CU(cudaMemGetInfo(free_bytes, total_bytes));
   return IRS_OK;
 }
 
@@ -540,6 +561,14 @@ int irs_sharedb_synth_db(irs_sharedb* const code_engines[3], irs_sharedb* const 
   return IRS_OK;
 }
 
+// Orders a write to an engine's query rows or records on stream s after the
+// last GEMM that read them (a direct launch, or a graph launch).
+static cudaError_t wait_last_dot(irs_sharedb* db, cudaStream_t s) {
+  cudaError_t e = cudaStreamWaitEvent(s, db->done, 0);
+  if (e != cudaSuccess) return e;
+  return cudaStreamWaitEvent(s, db->dm->graph_done, 0);
+}
+
 int irs_sharedb_query_upload(irs_sharedb* db, const uint16_t* rows, size_t n_rows) {
   CHECK(db && (rows || !n_rows), IRS_ERR_INVALID, "bad arguments");
   int rc = set_active_rows(db, n_rows);
@@ -547,6 +576,7 @@ int irs_sharedb_query_upload(irs_sharedb* db, const uint16_t* rows, size_t n_row
   irs_device_manager* dm = db->dm;
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = dm->streams[db->peer];
+  CU(wait_last_dot(db, s));  // the last GEMM has read the old limb planes
   const size_t K = db->code_length;
   CU(cudaMemsetAsync(db->q_stage, 0, db->n_pad * K * 2, s));
   if (n_rows) CU(cudaMemcpyAsync(db->q_stage, rows, n_rows * K * 2, cudaMemcpyHostToDevice, s));
@@ -572,6 +602,7 @@ int irs_sharedb_query_upload_slots(irs_sharedb* db, const uint16_t* base, size_t
   irs_device_manager* dm = db->dm;
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = dm->streams[db->peer];
+  CU(wait_last_dot(db, s));
   const size_t K = db->code_length;
   CU(cudaMemcpyAsync(db->q_stage, base, n_base * K * 2, cudaMemcpyHostToDevice, s));
   static_assert(sizeof(QuerySlot) == sizeof(irs_query_slot), "slot layout");
@@ -599,6 +630,7 @@ int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t 
   irs_device_manager* dm = db->dm;
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = dm->streams[db->peer];
+  CU(wait_last_dot(db, s));
   uint8_t* stage = reinterpret_cast<uint8_t*>(db->q_stage);
   const size_t table_off = (base_bytes + 15) / 16 * 16;
   CU(cudaMemcpyAsync(stage, base, base_bytes, cudaMemcpyHostToDevice, s));
@@ -606,6 +638,46 @@ int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t 
   CU(launch_expand_rows(db->q_stage, (uint32_t)K, reinterpret_cast<const uint32_t*>(stage + table_off), (uint32_t)n_rows,
                         (uint32_t)db->n_pad, db->q_lo, db->q_hi, s));
   CU(cudaStreamSynchronize(s));  // base / row_desc are caller-owned host memory
+  db->have_query = true;
+  return IRS_OK;
+}
+
+int irs_sharedb_query_put_base(irs_sharedb* db, size_t first, size_t n, const uint16_t* base) {
+  CHECK(db && (base || !n), IRS_ERR_INVALID, "bad arguments");
+  const size_t K = db->code_length;
+  CHECK((first + n) * K * 2 + db->n_cap * 4 + 16 <= db->n_cap * K * 2, IRS_ERR_INVALID,
+        "base queries [%zu, %zu) exceed the resident pool", first, first + n);
+  irs_device_manager* dm = db->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[db->peer];
+  if (n) {
+    CU(cudaMemcpyAsync(db->q_stage + first * K, base, n * K * 2, cudaMemcpyHostToDevice, s));
+    CU(cudaStreamSynchronize(s));  // caller-owned host memory
+  }
+  return IRS_OK;
+}
+
+int irs_sharedb_query_expand_rows(irs_sharedb* db, size_t n_base, const uint32_t* row_desc, size_t n_rows) {
+  CHECK(db && row_desc && n_base > 0, IRS_ERR_INVALID, "bad arguments");
+  CHECK(db->code_length % kRowLen == 0, IRS_ERR_INVALID, "rotations need code_length a multiple of 800");
+  const size_t K = db->code_length;
+  const size_t base_bytes = n_base * K * 2, table_bytes = n_rows * 4;
+  CHECK(base_bytes + table_bytes + 16 <= db->n_cap * K * 2, IRS_ERR_INVALID, "pool and row table exceed the staging");
+  for (size_t r = 0; r < n_rows; r++)
+    CHECK(row_desc[r] == 0xFFFFFFFFu || ((row_desc[r] >> 8) < n_base && (row_desc[r] & 0xFFu) < (uint32_t)kRotations),
+          IRS_ERR_INVALID, "row %zu descriptor 0x%x is invalid", r, row_desc[r]);
+  int rc = set_active_rows(db, n_rows);
+  if (rc) return rc;
+  irs_device_manager* dm = db->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[db->peer];
+  CU(wait_last_dot(db, s));
+  uint8_t* stage = reinterpret_cast<uint8_t*>(db->q_stage);
+  const size_t table_off = (base_bytes + 15) / 16 * 16;
+  CU(cudaMemcpyAsync(stage + table_off, row_desc, table_bytes, cudaMemcpyHostToDevice, s));
+  CU(launch_expand_rows(db->q_stage, (uint32_t)K, reinterpret_cast<const uint32_t*>(stage + table_off), (uint32_t)n_rows,
+                        (uint32_t)db->n_pad, db->q_lo, db->q_hi, s));
+  CU(cudaStreamSynchronize(s));  // row_desc is caller-owned host memory
   db->have_query = true;
   return IRS_OK;
 }
@@ -621,6 +693,7 @@ int irs_sharedb_gather_records(irs_sharedb* dst, irs_sharedb* src, const uint32_
   irs_device_manager* dm = dst->dm;
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = dm->streams[dst->peer];
+  CU(wait_last_dot(dst, s));  // the last GEMM over dst's records has finished
   const size_t K = dst->code_length;
   CHECK(n * 4 <= dst->n_cap * K * 2, IRS_ERR_INVALID, "too many records for one gather");
   // Staging reuse: the gather runs before the next query upload of `dst`.
@@ -704,7 +777,7 @@ int irs_sharedb_dot_many(irs_sharedb* const* engines, const uint16_t* multiplier
   for (int i = 0; i < n; i++) {
     engines[i]->res_offset = offset;
     engines[i]->res_len = len;
-    CU(cudaEventRecord(engines[i]->done, s));
+    if (!dm->capturing) CU(cudaEventRecord(engines[i]->done, s));  // a graph launch records graph_done instead
   }
   return IRS_OK;
 }
@@ -1105,6 +1178,7 @@ int irs_graph_end_capture(irs_device_manager* dm, irs_graph** out) {
     return fail(IRS_ERR_NOMEM, "host allocation failed");
   }
   gr->graph = g;
+  gr->dm = dm;
   cudaError_t e = cudaGraphInstantiate(&gr->exec, g, 0);
   if (e != cudaSuccess) {
     cudaGraphDestroy(g);
@@ -1118,6 +1192,8 @@ int irs_graph_end_capture(irs_device_manager* dm, irs_graph** out) {
 int irs_graph_launch(irs_graph* g, void* stream) {
   CHECK(g && g->exec, IRS_ERR_INVALID, "graph is NULL");
   CU(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+  // later query uploads on other party streams wait for the graph's GEMMs
+  CU(cudaEventRecord(g->dm->graph_done, static_cast<cudaStream_t>(stream)));
   return IRS_OK;
 }
 
@@ -1127,6 +1203,30 @@ int irs_graph_destroy(irs_graph* g) {
   if (g->graph) cudaGraphDestroy(g->graph);
   delete g;
   return IRS_OK;
+}
+
+int irs_dc_clear_rows(irs_distance_comparator* dc, size_t first, size_t n, void* stream) {
+  CHECK(dc && first + n <= dc->max_queries, IRS_ERR_INVALID, "rows out of range");
+  cudaStream_t s = party_stream(dc->dm, 0, stream);
+  const size_t words = dc->stride_bits / 32;
+  CU(cudaMemsetAsync(dc->bitmap + first * words, 0, n * words * 4, s));
+  return IRS_OK;
+}
+
+int irs_dc_fetch_rows(irs_distance_comparator* dc, size_t first, size_t n, uint32_t* host, size_t cap_words,
+                      size_t* row_words) {
+  CHECK(dc && host && row_words && first + n <= dc->max_queries, IRS_ERR_INVALID, "bad arguments");
+  const size_t words = dc->stride_bits / 32;
+  *row_words = words;
+  CHECK(n * words <= cap_words, IRS_ERR_INVALID, "host buffer holds %zu words, %zu needed", cap_words, n * words);
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[0];
+  if (n) {
+    CU(cudaMemcpyAsync(host, dc->bitmap + first * words, n * words * 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+  }
+  return check_device_error(dm);
 }
 
 int irs_dc_fetch_bitmap(irs_distance_comparator* dc, size_t n_queries, size_t db_len, uint64_t* host) {

@@ -57,6 +57,9 @@ _SIGS = {
     "irs_device_manager_error": [_vp, C.POINTER(_i)],
     "irs_device_manager_clear_error": [_vp],
     "irs_device_manager_sm_count": [_vp, C.POINTER(_i)],
+    "irs_device_manager_mem_info": [_vp, C.POINTER(_sz), C.POINTER(_sz)],
+    "irs_dc_clear_rows": [_vp, _sz, _sz, _vp],
+    "irs_dc_fetch_rows": [_vp, _sz, _sz, _vp, _sz, C.POINTER(_sz)],
     "irs_device_alloc": [_vp, _sz, C.POINTER(_vp)],
     "irs_device_free": [_vp, _vp],
     "irs_host_alloc_pinned": [_sz, C.POINTER(_vp)],
@@ -82,8 +85,11 @@ _SIGS = {
     "irs_sharedb_use_batch_counter": [_vp, _i],
     "irs_circuits_use_batch_counter": [_vp, _i],
     "irs_device_manager_set_batch_counter": [_vp, _u64, _vp],
+    "irs_device_manager_advance_batch_counter": [_vp, _vp],
     "irs_sharedb_query_upload_rows": [_vp, _vp, _sz, _vp, _sz],
     "irs_sharedb_gather_records": [_vp, _vp, _vp, _sz],
+    "irs_sharedb_query_put_base": [_vp, _sz, _sz, _vp],
+    "irs_sharedb_query_expand_rows": [_vp, _sz, _vp, _sz],
     "irs_mirror_query_share": [_vp, _sz, _i],
     "irs_dc_set_segments": [_vp, _sz, _vp, _vp, _vp],
     "irs_dc_compare_threshold_open_prepared": [_vp, _vp, _vp, _vp, _sz, _sz, _u32, _i, _vp],
@@ -301,6 +307,14 @@ class DeviceManager:
     def set_batch_counter(self, batch_id: int, stream=None) -> None:
         _check(lib().irs_device_manager_set_batch_counter(self.h, batch_id, stream))
 
+    def advance_batch_counter(self, stream=None) -> None:
+        _check(lib().irs_device_manager_advance_batch_counter(self.h, stream))
+
+    def mem_info(self):
+        f, t = _sz(), _sz()
+        _check(lib().irs_device_manager_mem_info(self.h, C.byref(f), C.byref(t)))
+        return f.value, t.value
+
     def sm_count(self) -> int:
         c = C.c_int()
         _check(lib().irs_device_manager_sm_count(self.h, C.byref(c)))
@@ -375,6 +389,16 @@ class ShareDB:
         b = np.ascontiguousarray(base, np.uint16).reshape(-1, self.code_length)
         rd = np.ascontiguousarray(row_desc, np.uint32)
         _check(lib().irs_sharedb_query_upload_rows(self.h, _ptr(b), b.shape[0], _ptr(rd), rd.size))
+
+    def query_put_base(self, first: int, base: np.ndarray) -> None:
+        """Writes base queries [first, first + len(base)) of the resident pool."""
+        b = np.ascontiguousarray(base, np.uint16).reshape(-1, self.code_length)
+        _check(lib().irs_sharedb_query_put_base(self.h, first, b.shape[0], _ptr(b)))
+
+    def query_expand_rows(self, n_base: int, row_desc) -> None:
+        """query_upload_rows over the resident pool [0, n_base)."""
+        rd = np.ascontiguousarray(row_desc, np.uint32)
+        _check(lib().irs_sharedb_query_expand_rows(self.h, n_base, _ptr(rd), rd.size))
 
     def gather_records(self, src: "ShareDB", ids) -> None:
         """prefetch_subset: records ids[k] of src become records k of this engine."""
@@ -496,6 +520,21 @@ class DistanceComparator:
         hm = (_vp * 3)(*[e.h for e in mask_engines])
         _check(lib().irs_dc_compare_threshold_open_prepared(self.h, circuits.h, C.cast(hc, _vp), C.cast(hm, _vp),
                                                             offset, length, threshold_a, int(self_check), stream))
+
+    def clear_rows(self, first: int, n: int, stream=None) -> None:
+        _check(lib().irs_dc_clear_rows(self.h, first, n, stream))
+
+    def fetch_rows(self, first: int, n: int, db_len: int) -> np.ndarray:
+        """Bitmap rows [first, first+n) unpacked to [n][db_len] uint8."""
+        stride = _sz()
+        probe = np.zeros(1, np.uint32)
+        _check(lib().irs_dc_fetch_rows(self.h, first, 0, _ptr(probe), 0, C.byref(stride)))
+        cap = max(n * stride.value, 1)
+        buf = np.zeros(cap, np.uint32)
+        _check(lib().irs_dc_fetch_rows(self.h, first, n, _ptr(buf), cap, C.byref(stride)))
+        rows = buf[: n * stride.value].reshape(n, stride.value)
+        bits = np.unpackbits(rows.view(np.uint8), axis=1, bitorder="little")
+        return bits[:, :db_len]
 
     def fetch_bitmap(self, n_queries: int, db_len: int) -> np.ndarray:
         """Reference layout: bit (q * db_len + e), u64 words."""

@@ -1,0 +1,95 @@
+"""Host-side logic of the continuous-batching server (no GPU): first-fit row
+placement inside 32-row words, the row/segment tables it produces, and the
+record split used by appends."""
+from __future__ import annotations
+
+import collections
+
+import numpy as np
+
+from irisb200.batched import centred_rotations
+from irisb200.serving import ContinuousServer, _first_run, _Variant, split_record_i8
+
+
+def test_first_run():
+    assert _first_run(0, 32) == 0
+    assert _first_run(0xFFFFFFFF, 1) == -1
+    assert _first_run(0x7FFFFFFF, 1) == 31
+    assert _first_run(0x7FFFFFFF, 2) == -1
+    assert _first_run(0x0000FFFF, 16) == 16
+    assert _first_run(0x00FF00FF, 8) == 8
+    assert _first_run(0x00FF00FF, 9) == -1
+    rng = np.random.default_rng(3)
+    for _ in range(2000):
+        occ = int(rng.integers(0, 1 << 32))
+        n = int(rng.integers(1, 33))
+        f = _first_run(occ, n)
+        runs = [s for s in range(33 - n) if all(not (occ >> (s + k)) & 1 for k in range(n))]
+        assert f == (runs[0] if runs else -1)
+
+
+def _placer(n_slots):
+    s = ContinuousServer.__new__(ContinuousServer)
+    s.n_slot_cap = n_slots
+    s.slot_occ = [0] * n_slots
+    s.slot_vars = [[] for _ in range(n_slots)]
+    return s
+
+
+def test_placement_and_tables():
+    s = _placer(4)
+    vs = []
+    for vid, n in enumerate([31, 16, 16, 1, 1, 31, 20]):
+        where = s._place(n)
+        assert where is not None
+        v = _Variant(vid, False, list(centred_rotations(n)))
+        s._occupy(v, *where)
+        vs.append(v)
+    assert [(v.slot, v.first) for v in vs] == [(0, 0), (1, 0), (1, 16), (0, 31), (2, 0), (2, 1), (3, 0)]
+    assert s._place(13) is None and s._place(12) == (3, 20)
+    row_desc, seg_start, seg_query, seg_mask = s._layout()
+    assert row_desc.size == 128
+    # every variant's rows carry its id and its centred rotations, and its segment mask covers exactly them
+    for v in vs:
+        rows = row_desc[v.slot * 32 + v.first: v.slot * 32 + v.first + len(v.rots)]
+        assert ((rows >> 8) == v.vid).all() and ((rows & 0xFF) == np.array(v.rots)).all()
+        segs = range(seg_start[v.slot], seg_start[v.slot + 1])
+        k = [j for j in segs if seg_query[j] == v.vid]
+        assert len(k) == 1 and seg_mask[k[0]] == (((1 << len(v.rots)) - 1) << v.first) & 0xFFFFFFFF
+    used = np.zeros(128, bool)
+    for v in vs:
+        used[v.slot * 32 + v.first: v.slot * 32 + v.first + len(v.rots)] = True
+    assert (row_desc[~used] == 0xFFFFFFFF).all()
+    # releasing frees exactly the rows; the table shrinks to the last used word
+    s._release(vs[6])
+    assert s.slot_occ[3] == 0
+    assert s._layout()[0].size == 96
+    assert s._place(31) == (3, 0)
+
+
+def test_admission_is_exact():
+    s = _placer(2)
+    s.free_variants = collections.deque(range(8))
+
+    class R:
+        kind = "uniqueness"
+        n_rot = 31
+        mirrored = True
+    assert s.can_admit(R())
+    R.n_rot = 17
+    assert s.can_admit(R())  # one word each
+    v = _Variant(0, False, list(range(17)))
+    s._occupy(v, 0, 0)
+    assert not s.can_admit(R())  # 15 rows left in word 0, one variant fits in word 1 only
+    R.mirrored = False
+    assert s.can_admit(R())
+    assert s.slot_occ == [(1 << 17) - 1, 0]  # the probe left no trace
+
+
+def test_split_record_i8_roundtrip():
+    rng = np.random.default_rng(5)
+    r = rng.integers(0, 65536, (2, 64)).astype(np.uint16)
+    lo, hi = split_record_i8(r)
+    assert lo.dtype == np.int8 and hi.dtype == np.int8
+    back = ((lo.view(np.uint8) ^ 0x80).astype(np.uint16) | ((hi.view(np.uint8) ^ 0x80).astype(np.uint16) << 8))
+    assert np.array_equal(back, r)

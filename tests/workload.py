@@ -69,3 +69,22 @@ def expected_bitmap(O, qc, qm, db_cs, db_ms, threshold_a, n_threads=0):
     q_mask = [rotated_rows(O, qm[p]) for p in range(3)]
     return O.cpu_plain_match(q_code, q_mask, nq, [db_cs[p] for p in range(3)], [db_ms[p] for p in range(3)],
                              threshold_a, n_threads)
+
+
+def expected_variant_hits(O, cs, ms, qc, qm, rotations, mirrored, entries, threshold_a):
+    """Entries matched by one query variant on the CPU: the per-party dots of
+    the variant's rotation rows (indices into all 31 rotations, 15 = centre)
+    against DB records `entries`, summed over parties (mask x2), thresholded,
+    OR over the rows.  qc [3][12800] / qm [3][6400] are the base query shares."""
+    base_c = [O.mirror_share(qc[p], True) if mirrored else qc[p] for p in range(3)]
+    base_m = [O.mirror_share(qm[p], False) if mirrored else qm[p] for p in range(3)]
+    entries = np.asarray(entries)
+    code = 0
+    mask = 0
+    for p in range(3):
+        rc = np.stack([O.rotate_share(base_c[p], r) for r in rotations])
+        rm = np.stack([O.rotate_share(base_m[p], r) for r in rotations])
+        code = code + O.dot_u16(rc, cs[p][entries]).astype(np.uint64)
+        mask = mask + 2 * O.dot_u16(rm, ms[p][entries]).astype(np.uint64)
+    hit = O.match_predicate(code % 65536, mask % 65536, threshold_a).max(axis=0)
+    return [int(e) for e, h in zip(entries, hit) if h]
