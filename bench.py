@@ -57,6 +57,12 @@ def parse():
     ap.add_argument("--threshold-a", type=int, default=16384)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cublas", action="store_true")
+    ap.add_argument("--mode", default="plain", choices=["plain", "serving"],
+                    help="plain: the drop-in batch (+ the batched uneven leg); serving: Poisson sweep")
+    ap.add_argument("--batched-requests", type=int, default=256, help="requests per batched-leg batch (0 = skip)")
+    ap.add_argument("--rates", default="50,200,500,1000,2000", help="serving: offered loads, requests/s")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: arrival window per load")
+    ap.add_argument("--chunk", type=int, default=65536, help="serving: DB chunk per step")
     return ap.parse_args()
 
 
@@ -201,6 +207,39 @@ def cublas_limb_gemms(torch, m, n_rows, warm=2, reps=3):
     return 3 * per_party
 
 
+def request_mix(n, code, mask, planted, db_len, seed, p_reauth=0.2, p_append=0.0):
+    """Requests of the batched/serving workloads: rotations 1/16/31 (uniform),
+    50% mirrored, p_reauth reauth (target = the planted entry of a planted
+    query, else a random entry), p_append appends; query j of the pool
+    (code/mask [3][nq][K]) is used cyclically."""
+    import numpy as np
+    from irisb200.batched import Request
+    rng = np.random.default_rng(seed)
+    nq = code.shape[1]
+    out = []
+    for i in range(n):
+        j = i % nq
+        u = rng.random()
+        if u < p_append:
+            out.append(Request(code=None, mask=None, kind="append"))
+            continue
+        kind = "reauth" if rng.random() < p_reauth else "uniqueness"
+        target = -1
+        if kind == "reauth":
+            target = planted[j][0] if j in planted else int(rng.integers(0, db_len))
+        out.append(Request(code=code[:, j], mask=mask[:, j], n_rot=int(rng.choice([1, 16, 31])),
+                           mirrored=bool(rng.random() < 0.5), kind=kind, target=target))
+    return out
+
+
+def comparisons_of(r, db_len):
+    """(query orientation, DB entry) pairs a request is compared on: a
+    uniqueness request scans the DB once per orientation, a reauth request
+    compares each orientation with its one target."""
+    k = 2 if r.mirrored else 1
+    return k * db_len if r.kind == "uniqueness" else k
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -239,8 +278,20 @@ def run_ours(args):
     A = args.threshold_a
     dm = irisb200.DeviceManager(local)
     seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
-    ce = [irisb200.ShareDB(p, dm, M, n_rows, K_CODE, seeds[p]) for p in range(3)]
-    me = [irisb200.ShareDB(p, dm, M, n_rows, K_MASK, seeds[p]) for p in range(3)]
+    # batched leg: its request mix, and the query rows of its packed uniqueness pass
+    reqs = None
+    q_cap = n_rows
+    if args.batched_requests and world == 1:
+        from irisb200.batched import centred_rotations, pack
+        nb = args.batched_requests
+        bpl = {j: (int((j * 104729 + 7) % M), (j * 5) % 31 - 15) for j in range(0, nb, 10)}
+        bc, bm = irisb200.synth_queries(DB_SEED + rank, Q_SEED + 1, nb, bpl)
+        reqs = request_mix(nb, bc, bm, bpl, M, seed=7)
+        lay = pack([list(centred_rotations(r.n_rot)) for r in reqs if r.kind == "uniqueness"
+                    for _ in range(2 if r.mirrored else 1)])
+        q_cap = max(n_rows, (lay.n_rows + 63) // 64 * 64)
+    ce = [irisb200.ShareDB(p, dm, M, q_cap, K_CODE, seeds[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, M, q_cap, K_MASK, seeds[p]) for p in range(3)]
     for e in ce + me:
         e.alloc_db(M)
     t0 = time.perf_counter()
@@ -340,12 +391,53 @@ def run_ours(args):
             e2e_step()
             lat.append((time.perf_counter() - ts) * 1e3)
         e2e_s = time.perf_counter() - t0
-    clk.__exit__(None, None, None)
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_value = comps * args.steps / e2e_s
+
+    # ---------------- batched uneven leg (same engines, same DB) ----------------
+    batched = None
+    if reqs:
+        from irisb200.batched import BatchedEngine
+        n_var = sum(2 if r.mirrored else 1 for r in reqs if r.kind == "uniqueness")
+        n_reauth = sum(2 if r.mirrored else 1 for r in reqs if r.kind == "reauth")
+        eng = BatchedEngine(dm, ce, me, c, max_variants=max(64, n_var), max_reauth=max(16, n_reauth),
+                            threshold_a=A, seeds=seeds, autotune=True)
+        for _ in range(max(2, args.warmup)):
+            eng.run(reqs)
+        dm.synchronize()
+        blat = []
+        with clk.mark():
+            tb = time.perf_counter()
+            for _ in range(args.steps):
+                ts = time.perf_counter()
+                bres = eng.run(reqs)
+                blat.append((time.perf_counter() - ts) * 1e3)
+            tb = time.perf_counter() - tb
+        bcomp = sum(comparisons_of(r, M) for r in reqs)
+        rows = sum(r.n_rot * (2 if r.mirrored else 1) for r in reqs if r.kind == "uniqueness")
+        tuned = {str(k): list(v) for k, v in eng.tuned.items()}
+        planted_hits = sum(1 for j, (e, _) in bpl.items()
+                           if reqs[j].kind == "uniqueness" and e in bres[j].matches)
+        planted_uniq = sum(1 for j in bpl if reqs[j].kind == "uniqueness")
+        eng.close()
+        batched = {
+            "value": bcomp * args.steps / tb, "unit": UNIT,
+            "vs_plain_e2e": (bcomp * args.steps / tb) / e2e_value,
+            "latency_ms": {"p50": sorted(blat)[len(blat) // 2], "p99": max(blat)},
+            "config": {"workload": f"batched uneven launches: {nb} requests per batch, rotations 1/16/31, "
+                                   "50% mirrored, 80% uniqueness (full DB) / 20% reauth (one target)",
+                       "uniqueness_orientations": n_var, "reauth_orientations": n_reauth,
+                       "uniqueness_query_rows": rows, "packed_rows": lay.n_rows, "comparisons_per_batch": bcomp,
+                       "autotuned_tile_chunk": tuned,
+                       "timing": "host wall clock per batch through BatchedEngine.run (H2D of the shares, "
+                                 "graph replay of the DB pass, reauth subset pass, D2H of the match lists)"},
+            "planted_matches_found": f"{planted_hits}/{planted_uniq}",
+            "clocks": clk.summary(clk.windows[-1]),
+        }
+    clk.__exit__(None, None, None)
 
     result = None
     if rank == 0:
@@ -390,6 +482,8 @@ def run_ours(args):
             "planted_matches_found": f"{planted_found}/{len(planted)}",
             "setup_s": {"synth_db": synth_s},
         }
+        if batched:
+            result["batched"] = batched
         mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
         if os.path.exists(mp):
             with open(mp) as f:
@@ -409,10 +503,126 @@ def run_ours(args):
     return result
 
 
+def _latency_stats(comps, requests, t0, db_lens):
+    lat = sorted((c.done - c.arrival) * 1e3 for c in comps if requests[c.idx].kind != "append")
+    if not lat:
+        return {}
+    end = max(c.done for c in comps)
+    work = sum(comparisons_of(requests[c.idx], db_lens[c.idx]) for c in comps if requests[c.idx].kind != "append")
+    return {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "max_ms": lat[-1], "mean_ms": statistics.mean(lat), "completed": len(comps),
+            "requests_per_s": len(comps) / (end - t0), "comparisons_per_s": work / (end - t0)}
+
+
+def run_serving(args):
+    """Poisson arrivals against the resident 512K-entry DB: the continuous
+    server and the plain batch-at-a-time drop-in at each offered load."""
+    import numpy as np
+    import torch
+
+    import irisb200
+    from irisb200.serving import ContinuousServer, PlainBatchServer, plan_row_capacity
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    torch.cuda.set_device(0)
+    M, A, chunk = args.db, args.threshold_a, args.chunk
+    dm = irisb200.DeviceManager(0)
+    seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
+    rates = [float(x) for x in args.rates.split(",") if x]
+    room = 64 + int(0.011 * max(rates) * args.serve_seconds * 2 * len(rates))
+    cap = M + room
+    # row capacity from the HBM left once the DB planes are resident (16 GB kept free)
+    free, _ = dm.mem_info()
+    db_bytes = cap * 3 * (K_CODE + K_MASK) * 2
+    R = min(8192, max(2048, ((free - db_bytes - (16 << 30)) // (chunk * 12 + 6 * 4 * K_CODE)) // 64 * 64))
+    ce = [irisb200.ShareDB(p, dm, chunk, R, K_CODE, seeds[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, chunk, R, K_MASK, seeds[p]) for p in range(3)]
+    for e in ce + me:
+        e.alloc_db(cap)
+    irisb200.synth_db(ce, me, DB_SEED, 0, M)
+    R_plan = plan_row_capacity(dm, chunk)
+    c = irisb200.Circuits(dm, seeds)
+    nq = 512
+    planted = {j: (int((j * 7919 + 13) % M), (j * 7) % 31 - 15) for j in range(0, nq, 10)}
+    qc, qm = irisb200.synth_queries(DB_SEED, Q_SEED + 2, nq, planted)
+    # append records: copies of existing irises (re-enrolments), fetched before any timing
+    app_ids = [int(x) for x in np.random.default_rng(3).integers(0, M, 64)]
+    app_c = np.stack([np.stack([ce[p].fetch_records(e, 1)[0] for e in app_ids]) for p in range(3)])  # [3][64][K]
+    app_m = np.stack([np.stack([me[p].fetch_records(e, 1)[0] for e in app_ids]) for p in range(3)])
+    max_var = min(R // 2, 4096)
+    srv = ContinuousServer(dm, ce, me, c, chunk=chunk, row_capacity=R, max_variants=max_var, max_reauth=64,
+                           threshold_a=A, seeds=seeds, db_capacity=cap)
+    plain = PlainBatchServer(dm, ce, me, c, chunk=chunk, max_slots=64, threshold_a=A, db_capacity=cap)
+    # warm both paths (kernels, graphs of nothing, allocator pools)
+    warm = request_mix(40, qc, qm, planted, M, seed=99)
+    srv.serve([0.0] * len(warm), warm)
+    plain.serve([0.0] * len(warm), warm)
+    clk = ClockSampler(0).__enter__()
+    time.sleep(2.0)
+    sweep = []
+    for li, lam in enumerate(rates):
+        rng = np.random.default_rng(1000 + li)
+        n = max(20, int(lam * args.serve_seconds))
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, n)).tolist()
+        reqs = request_mix(n, qc, qm, planted, M, seed=2000 + li, p_append=0.01)
+        appends = {i: (app_c[:, i % 64], app_m[:, i % 64]) for i, r in enumerate(reqs) if r.kind == "append"}
+        row = {"offered_requests_per_s": lam, "requests": n,
+               "appends": len(appends), "reauth": sum(r.kind == "reauth" for r in reqs)}
+        for name, server in (("served", srv), ("plain", plain)):
+            db0 = server.db_len
+            # each request's DB scope: the DB length after the appends that arrived before it
+            lens, cur = [], db0
+            for r in reqs:
+                if r.kind == "append":
+                    cur += 1
+                lens.append(cur)
+            steps0 = srv.steps
+            with clk.mark():
+                t0 = time.perf_counter()
+                comps = server.serve(arrivals, reqs, appends=appends, max_wall_s=300.0)
+            st = _latency_stats(comps, reqs, t0, lens)
+            st["clocks"] = clk.summary(clk.windows[-1])
+            if name == "served":
+                st["steps"] = srv.steps - steps0
+            row[name] = st
+        row["served_vs_plain_comparisons"] = row["served"]["comparisons_per_s"] / row["plain"]["comparisons_per_s"]
+        sweep.append(row)
+    clk.__exit__(None, None, None)
+    ok = [r for r in sweep if r["served"]["p99_ms"] < 1000]
+    okp = [r for r in sweep if r["plain"]["p99_ms"] < 1000]
+    best = max(ok, key=lambda r: r["served"]["comparisons_per_s"]) if ok else None
+    bestp = max(okp, key=lambda r: r["plain"]["comparisons_per_s"]) if okp else None
+    result = {
+        "metric": "iris comparisons/sec (3-party, 1 B200), continuous serving vs plain batch-at-a-time; "
+                  "p50/p99 request latency",
+        "value": best["served"]["comparisons_per_s"] if best else None, "unit": UNIT, "n_gpus": 1,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "plain_value": bestp["plain"]["comparisons_per_s"] if bestp else None,
+        "config": {"workload": f"serving: Poisson arrivals, {M} share-DB entries per party resident, 80% uniqueness "
+                               "/ 20% reauth, 1% appends, rotations 1/16/31, 50% mirrored",
+                   "row_capacity": R, "row_capacity_planned_from_free_hbm": R_plan, "chunk": chunk,
+                   "max_variants": max_var, "threshold_a": A, "serve_seconds": args.serve_seconds,
+                   "value_rule": "highest comparisons/s over the offered loads whose p99 latency is below 1 s",
+                   "comparison": "one (query orientation, DB entry) pair; a reauth orientation is one comparison",
+                   "plain": "batches of up to 64 orientations x 31 rotations, whole DB per batch, FIFO"},
+        "sweep": sweep,
+    }
+    print(json.dumps(result), flush=True)
+    srv.close()
+    plain.close()
+    for o in ce + me + [c]:
+        o.close()
+    dm.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

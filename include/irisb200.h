@@ -296,6 +296,14 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
                                            irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3],
                                            size_t offset, size_t len, uint32_t threshold_a, int self_check,
                                            void* stream);
+/* Match lists of selected bitmap rows (the per-query assembly of
+ * fetch_final_results, distance_comparator.rs, for rows chosen by the caller):
+ * counts[i] = set bits of row rows[i] below db_len, ids [n][IRS_MAX_MATCHES_LEN]
+ * = the lowest min(counts[i], 256) of those entries in ascending order.  With
+ * clear != 0 the rows are zeroed in the same pass (a serving loop reusing the
+ * rows of completed requests).  Synchronous. */
+int irs_dc_take_rows(irs_distance_comparator* dc, const uint32_t* rows, size_t n, size_t db_len, int clear,
+                     uint32_t* counts, uint32_t* ids);
 /* Clears bitmap rows [first, first + n) (a query row reused by the serving
  * loop for a new request). */
 int irs_dc_clear_rows(irs_distance_comparator* dc, size_t first, size_t n, void* stream);

@@ -120,6 +120,7 @@ struct irs_distance_comparator {
   uint32_t* all_matches = nullptr;    // [max_queries][256]
   uint32_t* d_slot_valid = nullptr;
   uint32_t* d_slot_query = nullptr;
+  uint32_t* d_take = nullptr;  // irs_dc_take_rows: row list [max_queries], counts [max_queries], ids [max_queries][256]
   size_t slot_cap = 0;
   // segment table (irs_dc_set_segments)
   uint32_t* d_seg_start = nullptr;  // [slot_cap + 1]
@@ -982,6 +983,7 @@ int irs_dc_init(irs_device_manager* dm, size_t max_queries, size_t max_db_length
       {(void**)&dc->d_seg_start, (dc->slot_cap + 1) * 4},
       {(void**)&dc->d_seg_query, dc->slot_cap * 32 * 4},
       {(void**)&dc->d_seg_mask, dc->slot_cap * 32 * 4},
+      {(void**)&dc->d_take, max_queries * (2 + kMaxMatchesLen) * 4},
   };
   for (auto& a : allocs) {
     cudaError_t e = cudaMalloc(a.p, a.bytes);
@@ -1003,7 +1005,7 @@ int irs_dc_destroy(irs_distance_comparator* dc) {
   cudaSetDevice(dc->dm->device);
   void* ps[] = {dc->bitmap, dc->self_bitmap, dc->match_list, dc->counters, dc->partial, dc->final_results,
                 dc->match_counters, dc->all_matches, dc->d_slot_valid, dc->d_slot_query,
-                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask};
+                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask, dc->d_take};
   for (void* p : ps) if (p) cudaFree(p);
   delete dc;
   return IRS_OK;
@@ -1043,7 +1045,9 @@ int irs_dc_compare_threshold_open(irs_distance_comparator* dc, irs_circuits* c, 
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = party_stream(dm, 0, stream);
   // Receive: wait until every party's shares have been produced.
-  for (int p = 0; p < 3; p++) {
+  // The GEMMs ran on another stream: wait for them (inside a graph capture
+  // they are earlier nodes of the same capture stream).
+  for (int p = 0; !dm->capturing && p < 3; p++) {
     CU(cudaStreamWaitEvent(s, code_engines[p]->done, 0));
     CU(cudaStreamWaitEvent(s, mask_engines[p]->done, 0));
   }
@@ -1126,7 +1130,9 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
   irs_device_manager* dm = dc->dm;
   CU(cudaSetDevice(dm->device));
   cudaStream_t s = party_stream(dm, 0, stream);
-  for (int p = 0; p < 3; p++) {
+  // The GEMMs ran on another stream: wait for them (inside a graph capture
+  // they are earlier nodes of the same capture stream).
+  for (int p = 0; !dm->capturing && p < 3; p++) {
     CU(cudaStreamWaitEvent(s, code_engines[p]->done, 0));
     CU(cudaStreamWaitEvent(s, mask_engines[p]->done, 0));
   }
@@ -1203,6 +1209,29 @@ int irs_graph_destroy(irs_graph* g) {
   if (g->graph) cudaGraphDestroy(g->graph);
   delete g;
   return IRS_OK;
+}
+
+int irs_dc_take_rows(irs_distance_comparator* dc, const uint32_t* rows, size_t n, size_t db_len, int clear,
+                     uint32_t* counts, uint32_t* ids) {
+  CHECK(dc && (n == 0 || (rows && counts && ids)), IRS_ERR_INVALID, "bad arguments");
+  CHECK(n <= dc->max_queries, IRS_ERR_INVALID, "%zu rows exceed the comparator's %zu", n, dc->max_queries);
+  CHECK(db_len <= dc->stride_bits, IRS_ERR_INVALID, "db_len %zu exceeds the bitmap width", db_len);
+  for (size_t i = 0; i < n; i++)
+    CHECK(rows[i] < dc->max_queries, IRS_ERR_INVALID, "row %u out of range", rows[i]);
+  if (!n) return IRS_OK;
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[0];
+  uint32_t* d_rows = dc->d_take;
+  uint32_t* d_counts = d_rows + dc->max_queries;
+  uint32_t* d_ids = d_counts + dc->max_queries;
+  CU(cudaMemcpyAsync(d_rows, rows, n * 4, cudaMemcpyHostToDevice, s));
+  CU(launch_take_rows(dc->bitmap, (uint32_t)(dc->stride_bits / 32), d_rows, (uint32_t)n, (uint32_t)db_len, clear,
+                      d_counts, d_ids, kMaxMatchesLen, s));
+  CU(cudaMemcpyAsync(counts, d_counts, n * 4, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(ids, d_ids, n * kMaxMatchesLen * 4, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return check_device_error(dm);
 }
 
 int irs_dc_clear_rows(irs_distance_comparator* dc, size_t first, size_t n, void* stream) {

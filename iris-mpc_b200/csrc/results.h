@@ -16,4 +16,8 @@ cudaError_t launch_merge_batch(const uint32_t* left, const uint32_t* right, uint
                                uint32_t* final_results, uint32_t* match_counter, uint32_t* all_matches,
                                cudaStream_t stream);
 
+cudaError_t launch_take_rows(uint32_t* bitmap, uint32_t stride_words, const uint32_t* rows, uint32_t n_rows,
+                             uint32_t db_len, int clear, uint32_t* counts, uint32_t* ids, uint32_t cap,
+                             cudaStream_t stream);
+
 }  // namespace irs

@@ -59,6 +59,7 @@ _SIGS = {
     "irs_device_manager_sm_count": [_vp, C.POINTER(_i)],
     "irs_device_manager_mem_info": [_vp, C.POINTER(_sz), C.POINTER(_sz)],
     "irs_dc_clear_rows": [_vp, _sz, _sz, _vp],
+    "irs_dc_take_rows": [_vp, _vp, _sz, _sz, _i, _vp, _vp],
     "irs_dc_fetch_rows": [_vp, _sz, _sz, _vp, _sz, C.POINTER(_sz)],
     "irs_device_alloc": [_vp, _sz, C.POINTER(_vp)],
     "irs_device_free": [_vp, _vp],
@@ -520,6 +521,15 @@ class DistanceComparator:
         hm = (_vp * 3)(*[e.h for e in mask_engines])
         _check(lib().irs_dc_compare_threshold_open_prepared(self.h, circuits.h, C.cast(hc, _vp), C.cast(hm, _vp),
                                                             offset, length, threshold_a, int(self_check), stream))
+
+    def take_rows(self, rows, db_len: int, clear: bool = True):
+        """(counts [n], ids [n][256]) of the listed bitmap rows; see irs_dc_take_rows."""
+        r = np.ascontiguousarray(rows, np.uint32)
+        counts = np.zeros(max(r.size, 1), np.uint32)
+        ids = np.zeros((max(r.size, 1), MAX_MATCHES_LEN), np.uint32)
+        _check(lib().irs_dc_take_rows(self.h, _ptr(r) if r.size else None, r.size, db_len, int(clear), _ptr(counts),
+                                      _ptr(ids)))
+        return counts[: r.size], ids[: r.size]
 
     def clear_rows(self, first: int, n: int, stream=None) -> None:
         _check(lib().irs_dc_clear_rows(self.h, first, n, stream))

@@ -28,6 +28,7 @@ admitted afterwards scan it.  The device batch counter advances every step
 from __future__ import annotations
 
 import collections
+import heapq
 import math
 import time
 from dataclasses import dataclass, field
@@ -123,7 +124,8 @@ class ContinuousServer:
         self.db_capacity = db_capacity or self.db_len
         self.dc = DistanceComparator(dm, max_variants, max(self.db_capacity, 64), match_list_cap=1 << 16)
         self.dc.reset()
-        self.free_variants = collections.deque(range(max_variants))
+        self.free_variants = list(range(max_variants))  # min-heap: low ids keep pool writes contiguous
+        self.pending_bases = {}  # vid -> (code [3][12800], mask [3][6400]) not yet in the device pool
         seeds = seeds or [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
         self.max_reauth = max_reauth
         nsub = 2 * max_reauth
@@ -190,17 +192,15 @@ class ContinuousServer:
         the resident pool (pool index = bitmap row)."""
         variants = []
         for mir in ([False, True] if r.mirrored else [False]):
-            v = _Variant(self.free_variants.popleft(), mir, list(centred_rotations(r.n_rot)))
             where = self._place(r.n_rot)
             if where is None:
                 raise RuntimeError("admit() without room: call can_admit() first")
+            v = _Variant(heapq.heappop(self.free_variants), mir, list(centred_rotations(r.n_rot)))
             self._occupy(v, *where)
             variants.append(v)
-            for p in range(3):
-                code = mirror_query_share(r.code[p], True) if mir else r.code[p]
-                mask = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
-                self.ce[p].query_put_base(v.vid, code[None])
-                self.me[p].query_put_base(v.vid, mask[None])
+            code = np.stack([mirror_query_share(r.code[p], True) if mir else r.code[p] for p in range(3)])
+            mask = np.stack([mirror_query_share(r.mask[p], False) if mir else r.mask[p] for p in range(3)])
+            self.pending_bases[v.vid] = (code, mask)
         f = _Flight(r, idx, arrival, self.db_len, variants, set(range(math.ceil(self.db_len / self.chunk))))
         self.flight.append(f)
         self.layout_dirty = True
@@ -220,7 +220,25 @@ class ContinuousServer:
             seg_start.append(len(seg_query))
         return row_desc, np.array(seg_start, np.uint32), np.array(seg_query, np.uint32), np.array(seg_mask, np.uint32)
 
+    def _flush_bases(self) -> None:
+        """Writes the newly admitted variants' base shares into the device
+        pool, one copy per engine per contiguous run of pool indices."""
+        vids = sorted(self.pending_bases)
+        runs, start = [], 0
+        for i in range(1, len(vids) + 1):
+            if i == len(vids) or vids[i] != vids[i - 1] + 1:
+                runs.append(vids[start:i])
+                start = i
+        for run in runs:
+            code = np.stack([self.pending_bases[v][0] for v in run], axis=1)  # [3][n][12800]
+            mask = np.stack([self.pending_bases[v][1] for v in run], axis=1)
+            for p in range(3):
+                self.ce[p].query_put_base(run[0], code[p])
+                self.me[p].query_put_base(run[0], mask[p])
+        self.pending_bases.clear()
+
     def _upload_layout(self) -> None:
+        self._flush_bases()
         row_desc, seg_start, seg_query, seg_mask = self._layout()
         for e in self.ce + self.me:
             e.query_expand_rows(self.max_variants, row_desc)
@@ -284,21 +302,28 @@ class ContinuousServer:
 
     # -- the chunk step -------------------------------------------------------------
     def _finish(self, done: list) -> list:
-        self.dm.synchronize()
+        """Match lists of the completed requests' bitmap rows (one compaction
+        launch per distinct DB snapshot), rows cleared for reuse."""
+        by_len = collections.defaultdict(list)
+        for f in done:
+            for v in f.variants:
+                by_len[f.db_len].append(v)
+        hits = {}
+        for db_len, vs in by_len.items():
+            counts, ids = self.dc.take_rows([v.vid for v in vs], db_len, clear=True)
+            for v, n, row in zip(vs, counts, ids):
+                hits[v.vid] = row[: min(int(n), len(row))].tolist()
         now = time.perf_counter()
         out = []
         for f in done:
             res = Result()
             for v in f.variants:
-                row = self.dc.fetch_rows(v.vid, 1, f.db_len)[0] if f.db_len else np.zeros(0, np.uint8)
-                hits = np.nonzero(row)[0].tolist()
                 if v.mirrored:
-                    res.mirror_matches = hits
+                    res.mirror_matches = hits[v.vid]
                 else:
-                    res.matches = hits
-                self.dc.clear_rows(v.vid, 1)
+                    res.matches = hits[v.vid]
                 self._release(v)
-                self.free_variants.append(v.vid)
+                heapq.heappush(self.free_variants, v.vid)
             out.append(Completion(f.idx, f.arrival, now, res))
         self.layout_dirty = True
         return out
@@ -371,3 +396,126 @@ class ContinuousServer:
     def close(self) -> None:
         for o in self.sce + self.sme + [self.dc, self.sdc]:
             o.close()
+
+
+class PlainBatchServer:
+    """The plain drop-in served one batch at a time, as the reference's actor
+    does (actor.rs:584-644): the requests that have arrived are taken in
+    order, every orientation of every request (reauth included) gets one
+    32-row slot with all 31 rotations, the whole DB is scanned chunk by chunk
+    for the batch, and all its requests complete together.  A batch holds up
+    to `max_slots` orientations (64 in the plain drop-in)."""
+
+    def __init__(self, dm, code_engines, mask_engines, circuits, chunk: int = 65536, max_slots: int = 64,
+                 threshold_a: int = 16384, db_capacity: int | None = None):
+        self.dm = dm
+        self.ce, self.me = list(code_engines), list(mask_engines)
+        self.c = circuits
+        self.A = threshold_a
+        self.chunk = chunk
+        self.max_slots = max_slots
+        self.db_capacity = db_capacity or self.ce[0].db_len()
+        self.dc = DistanceComparator(dm, max_slots, max(self.db_capacity, 64), match_list_cap=1 << 16)
+        for e in self.ce + self.me:
+            e.use_batch_counter(True)  # fresh ChaCha batch id per chunk from the device counter
+        circuits.use_batch_counter(True)
+        self.batches = 0
+
+    @property
+    def db_len(self) -> int:
+        return self.ce[0].db_len()
+
+    def append(self, code_records: np.ndarray, mask_records: np.ndarray) -> int:
+        idx = self.db_len
+        if idx >= self.db_capacity:
+            raise ValueError("DB capacity exhausted")
+        for p in range(3):
+            self.ce[p].load_records_i8(idx, *split_record_i8(code_records[p][None]))
+            self.me[p].load_records_i8(idx, *split_record_i8(mask_records[p][None]))
+            self.ce[p].set_db_len(idx + 1)
+            self.me[p].set_db_len(idx + 1)
+        return idx
+
+    def run_batch(self, items) -> list:
+        """items: [(idx, arrival, Request)] of uniqueness/reauth requests."""
+        variants = [(j, mir) for j, (_, _, r) in enumerate(items) for mir in ([False, True] if r.mirrored else [False])]
+        if len(variants) > self.max_slots:
+            raise ValueError("batch exceeds the slot capacity")
+        base_c = np.zeros((3, len(variants), IRIS_CODE_LENGTH), np.uint16)
+        base_m = np.zeros((3, len(variants), MASK_CODE_LENGTH), np.uint16)
+        for v, (j, mir) in enumerate(variants):
+            r = items[j][2]
+            for p in range(3):
+                base_c[p, v] = mirror_query_share(r.code[p], True) if mir else r.code[p]
+                base_m[p, v] = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
+        slots = [(v, 0, 31, v) for v in range(len(variants))]
+        for p in range(3):
+            self.ce[p].query_upload_slots(base_c[p], slots)
+            self.me[p].query_upload_slots(base_m[p], slots)
+        db_len = self.db_len
+        self.dc.reset()
+        for off in range(0, db_len, self.chunk):
+            ln = min(self.chunk, db_len - off)
+            self.dm.advance_batch_counter()
+            dot_many(self.ce + self.me, MULTS, off, ln)
+            self.dc.compare_threshold_open(self.c, self.ce, self.me, off, ln, len(variants), self.A)
+        counts, ids = self.dc.take_rows(list(range(len(variants))), db_len, clear=False)
+        rows = None
+        if any(r.kind == "reauth" for _, _, r in items):
+            rows = self.dc.fetch_rows(0, len(variants), db_len)
+        now = time.perf_counter()
+        out = {j: Result() for j in range(len(items))}
+        for v, (j, mir) in enumerate(variants):
+            r = items[j][2]
+            if r.kind == "reauth":
+                hit = bool(rows[v, r.target])
+                if mir:
+                    out[j].reauth_mirror_match = hit
+                else:
+                    out[j].reauth_match = hit
+            else:
+                hits = ids[v, : min(int(counts[v]), ids.shape[1])].tolist()
+                if mir:
+                    out[j].mirror_matches = hits
+                else:
+                    out[j].matches = hits
+        self.batches += 1
+        return [Completion(items[j][0], items[j][1], now, out[j]) for j in range(len(items))]
+
+    def serve(self, arrivals, requests, appends=None, max_wall_s: float = 600.0) -> list:
+        """Open-loop run with the arrivals of ContinuousServer.serve."""
+        t0 = time.perf_counter()
+        order = collections.deque(sorted(range(len(requests)), key=lambda i: arrivals[i]))
+        completions = []
+        while order:
+            now = time.perf_counter() - t0
+            if now > max_wall_s:
+                raise TimeoutError("serving run exceeded its wall-clock budget")
+            if arrivals[order[0]] > now:
+                time.sleep(max(0.0, min(0.002, arrivals[order[0]] - now)))
+                continue
+            items, used = [], 0
+            while order and arrivals[order[0]] <= now:
+                i = order[0]
+                r = requests[i]
+                if r.kind == "append":
+                    if items:
+                        break  # appends take effect between batches, in arrival order
+                    order.popleft()
+                    code, mask = appends[i]
+                    self.append(code, mask)
+                    completions.append(Completion(i, t0 + arrivals[i], time.perf_counter(), Result()))
+                    continue
+                need = 2 if r.mirrored else 1
+                if used + need > self.max_slots:
+                    break
+                order.popleft()
+                items.append((i, t0 + arrivals[i], r))
+                used += need
+            if items:
+                completions += self.run_batch(items)
+        self.dm.synchronize()
+        return completions
+
+    def close(self) -> None:
+        self.dc.close()
