@@ -12,19 +12,9 @@ for p in (ROOT, PKG):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE = "/root/reference"
-
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 and the built CUDA library")
-
-
-def reference_file(rel: str) -> str:
-    """Path of a reference data file; skips the test when the reference tree is absent."""
-    path = os.path.join(REFERENCE, rel)
-    if not os.path.exists(path):
-        pytest.skip(f"reference data {rel} not available on this machine")
-    return path
 
 
 @pytest.fixture(scope="session")

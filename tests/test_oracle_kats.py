@@ -7,13 +7,19 @@ galois_engine.rs:784-867 (hamming_distance_galois, random_codes.txt),
 galois_engine.rs:938-996 and iris.rs:742-766 (mirrored codes,
 flipped_codes.txt), iris.rs:726-741 (decode_from_string, all_rotations.txt),
 galois_engine.rs:998-1013 (check_remap), threshold.rs:110-124 (real_result_msb).
+The example-data vectors come from tests/golden/reference_kats.json, written
+from the reference's example-data files by tests/golden/make_golden.py.
 """
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
-from conftest import reference_file
+import hashlib
+import json
+import os
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_kats.json")))
 
 S64 = [
     [1, 0, 0, 0],
@@ -97,10 +103,6 @@ def test_rotation_aware_dot_trick(oracle):
         assert dot == (mc - 2 * hd) % 65536
 
 
-def _lines(path):
-    return [ln.strip() for ln in open(path) if ln.strip()]
-
-
 def _calc_distance(oracle, code_sh, mask_sh, q_code_sh, q_mask_sh):
     """calculate_distance (galois_engine.rs:869-913)."""
     cd = sum(oracle.trick_dot(code_sh[p], oracle.preprocess_query(p, q_code_sh[p])) for p in range(3)) % 65536
@@ -110,9 +112,9 @@ def _calc_distance(oracle, code_sh, mask_sh, q_code_sh, q_mask_sh):
 
 
 def test_hamming_distance_galois(oracle):
-    lines = _lines(reference_file("iris-mpc-common/src/example-data/random_codes.txt"))
-    c1, m1, c2, m2 = (oracle.iris_from_base64(x) for x in lines[:4])
-    d0, d15 = float(lines[4]), float(lines[5])
+    g = GOLDEN["random_codes"]
+    c1, m1, c2, m2 = (oracle.iris_from_base64(g[k]) for k in ("code1", "mask1", "code2", "mask2"))
+    d0, d15 = g["distance_rot0"], g["distance_min_rot"]
     assert abs(oracle.fractional_distance(c1, m1, c2, m2) - d0) <= 1e-6
     t1c = oracle.encode_iris_code(c1, m1, 21)
     t1m = oracle.encode_mask_code(m1, 22)
@@ -128,8 +130,9 @@ def test_hamming_distance_galois(oracle):
 
 
 def test_match_mirrored_codes(oracle):
-    lines = _lines(reference_file("iris-mpc-common/src/example-data/flipped_codes.txt"))
-    code, mask, fcode, fmask = (oracle.iris_from_base64(x) for x in lines[:4])
+    g = GOLDEN["flipped_codes"]
+    code, mask, fcode, fmask = (oracle.iris_from_base64(g[k]) for k in ("code", "mask", "flipped_code",
+                                                                         "flipped_mask"))
     mask_both = mask & fmask
     plain = oracle.fractional_distance(code, mask_both, fcode, fmask)
     cs = oracle.encode_iris_code(code, mask_both, 31)
@@ -147,19 +150,14 @@ def test_match_mirrored_codes(oracle):
 
 
 def test_decode_and_rotations(oracle):
-    path = reference_file("iris-mpc-common/src/example-data/all_rotations.txt")
-    lines = _lines(path)
-    code = oracle.iris_from_base64(lines[0])
-    rots = {}
-    for ln in lines[1:]:
-        k, v = ln.split(":", 1)
-        rots[int(k)] = v.replace(" ", "").strip()
-    bits = "".join(str(b) for b in oracle.bits_of(code))
-    assert bits == rots[0]
-    assert oracle.iris_to_base64(code) == lines[0]
+    g = GOLDEN["all_rotations"]
+    code = oracle.iris_from_base64(g["code"])
+    assert oracle.iris_to_base64(code) == g["code"]
+    rots = {int(k): v for k, v in g["rotation_bits_sha256"].items()}
+    assert sorted(rots) == list(range(-15, 16))
     for r, expect in rots.items():
         got = "".join(str(b) for b in oracle.bits_of(oracle.iris_rotate(code, r)))
-        assert got == expect, f"rotation {r}"
+        assert hashlib.sha256(got.encode()).hexdigest() == expect, f"rotation {r}"
 
 
 def test_remap_roundtrip(oracle):
