@@ -92,6 +92,34 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// The same copy with an L2 eviction-priority policy (createpolicy).
+__device__ __forceinline__ void tma_load_2d_hint(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y,
+                                                 uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint64_t policy_evict_normal() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
 // 1024 bytes apart (SBO), version 1, layout type 2 (SWIZZLE_128B).
 __device__ __forceinline__ uint64_t smem_desc(const void* p) {
@@ -219,6 +247,9 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
       bool issued[8];
       for (int s = 0; s < C::kStages; s++) issued[s] = false;
       bool ok = true;
+      const bool hinted = P.l2_hint != 0;
+      const uint64_t pol_a = (P.l2_hint & 2u) ? policy_evict_first() : policy_evict_normal();
+      const uint64_t pol_b = (P.l2_hint & 1u) ? policy_evict_last() : policy_evict_normal();
       for (int t = blockIdx.x; ok && t < P.total_tiles; t += gridDim.x) {
         Tile tl;
         if (!tile_of(P, t, tl)) break;
@@ -229,10 +260,17 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
           if (!mbar_wait(&empty_bar[stage], phase ^ 1u, err, kErrTimeoutEmpty)) { ok = false; break; }
           mbar_expect_tx(&full_bar[stage], (uint32_t)C::kStageBytes);
           const int x = (int)ki * kBK;
-          tma_load_2d(a_lo + stage * kBM * kBK, &pr.tm_a_lo, &full_bar[stage], x, ya);
-          tma_load_2d(a_hi + stage * kBM * kBK, &pr.tm_a_hi, &full_bar[stage], x, ya);
-          tma_load_2d(b_lo + stage * BN * kBK, &pr.tm_b_lo, &full_bar[stage], x, yb);
-          tma_load_2d(b_hi + stage * BN * kBK, &pr.tm_b_hi, &full_bar[stage], x, yb);
+          if (hinted) {
+            tma_load_2d_hint(a_lo + stage * kBM * kBK, &pr.tm_a_lo, &full_bar[stage], x, ya, pol_a);
+            tma_load_2d_hint(a_hi + stage * kBM * kBK, &pr.tm_a_hi, &full_bar[stage], x, ya, pol_a);
+            tma_load_2d_hint(b_lo + stage * BN * kBK, &pr.tm_b_lo, &full_bar[stage], x, yb, pol_b);
+            tma_load_2d_hint(b_hi + stage * BN * kBK, &pr.tm_b_hi, &full_bar[stage], x, yb, pol_b);
+          } else {
+            tma_load_2d(a_lo + stage * kBM * kBK, &pr.tm_a_lo, &full_bar[stage], x, ya);
+            tma_load_2d(a_hi + stage * kBM * kBK, &pr.tm_a_hi, &full_bar[stage], x, ya);
+            tma_load_2d(b_lo + stage * BN * kBK, &pr.tm_b_lo, &full_bar[stage], x, yb);
+            tma_load_2d(b_hi + stage * BN * kBK, &pr.tm_b_hi, &full_bar[stage], x, yb);
+          }
           issued[stage] = true;
           issued_phase[stage] = (int)phase;
           if (++stage == C::kStages) { stage = 0; phase ^= 1u; }
@@ -718,8 +756,24 @@ int gemm_block_n_for(uint32_t n_pad) {
   return 0;
 }
 
+// L2 policy of the one-SM kernel's loads (GemmParams::l2_hint), opt-in through
+// IRS_GEMM_L2HINT.  Measured at 524,288 entries x 2048 query rows: the query
+// planes are re-read from DRAM once per sweep of the 148 CTAs over the DB
+// (about 1.8x the algorithmic bytes in all), but DRAM runs at ~16% of its
+// bandwidth under this tensor-bound kernel, and keeping the queries with
+// evict_last saved 2% of the traffic while slowing the GEMM by 3% and the
+// following threshold kernel by 18% (the pinned lines outlive the GEMM).
+static uint32_t gemm_l2_hint() {
+  static const uint32_t hint = [] {
+    const char* e = getenv("IRS_GEMM_L2HINT");
+    return e ? (uint32_t)atoi(e) & 3u : 0u;
+  }();
+  return hint;
+}
+
 cudaError_t launch_limb_gemm(GemmParams& P, int block_n, int n_sms, cudaStream_t stream) {
   const bool pair = gemm_use_pair(block_n);
+  P.l2_hint = gemm_l2_hint();
   const uint32_t bm = pair ? (uint32_t)kBM2 : (uint32_t)kBM;
   P.total_tiles = 0;
   for (int i = 0; i < P.n_prob; i++) {

@@ -37,6 +37,9 @@ struct GemmParams {
   int n_prob;
   int total_tiles;
   int* err;
+  // L2 eviction priority of the TMA loads: bit 0 = query planes evict_last
+  // (re-read by every DB tile), bit 1 = DB planes evict_first (streamed).
+  uint32_t l2_hint;
 };
 
 // Builds a 2-D u8 tensor map (inner dim K, outer dim rows) with 128x`box_rows`
