@@ -22,8 +22,10 @@ CPU path (per-party rotation-aware dots, summed, thresholded, OR over
 rotations) on the host cores.
 
 Multi-GPU (torchrun): each rank hosts its own 524,288-entry shard of all three
-parties and processes the same query batch; no data-path collective (weak
-scaling); the max step time over ranks is reported.
+parties (global entry g on rank g % N) and processes the same query batch; the
+scan needs no collective (weak scaling); the end-to-end step merges the ranks'
+match results with one all_gather (irisb200.shard); the max step time over
+ranks is reported.
 """
 from __future__ import annotations
 
@@ -376,7 +378,11 @@ def run_ours(args):
         irisb200.dot_many(engines, mults, 0, M)
         dc.compare_threshold_open(c, ce, me, 0, M, NQ, A)
         dc.join_db_matches(NQ, M)
-        return dc.fetch_final_results(NQ)
+        res = dc.fetch_final_results(NQ)
+        if dist:  # merge the shards' results (get_merged_results over ranks): one all_gather
+            from irisb200.shard import exchange_results
+            return exchange_results(*res, device=torch.device("cuda", local))
+        return res
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
