@@ -67,9 +67,9 @@ def _rank(rank, world, port, out):
 def test_sharded_scan_merges_to_the_unsharded_result():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
         out = m.dict()
-        ctx = mp.get_context("spawn")
         procs = [ctx.Process(target=_rank, args=(r, world, port, out)) for r in range(world)]
         for p in procs:
             p.start()
