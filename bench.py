@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--rates", default="50,200,500,1000,2000", help="serving: offered loads, requests/s")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: arrival window per load")
     ap.add_argument("--chunk", type=int, default=65536, help="serving: DB chunk per step")
+    ap.add_argument("--serving-arms", default="served,plain", help="serving: which servers to run")
     return ap.parse_args()
 
 
@@ -588,7 +589,8 @@ def run_serving(args):
         appends = {i: (app_c[:, i % 64], app_m[:, i % 64]) for i, r in enumerate(reqs) if r.kind == "append"}
         row = {"offered_requests_per_s": lam, "requests": n,
                "appends": len(appends), "reauth": sum(r.kind == "reauth" for r in reqs)}
-        for name, server in (("served", srv), ("plain", plain)):
+        arms = [a for a in (("served", srv), ("plain", plain)) if a[0] in args.serving_arms.split(",")]
+        for name, server in arms:
             db0 = server.db_len
             # each request's DB scope: the DB length after the appends that arrived before it
             lens, cur = [], db0
@@ -596,20 +598,29 @@ def run_serving(args):
                 if r.kind == "append":
                     cur += 1
                 lens.append(cur)
-            steps0 = srv.steps
+            stats0 = dict(srv.stats)
             with clk.mark():
                 t0 = time.perf_counter()
                 comps = server.serve(arrivals, reqs, appends=appends, max_wall_s=300.0)
             st = _latency_stats(comps, reqs, t0, lens)
             st["clocks"] = clk.summary(clk.windows[-1])
             if name == "served":
-                st["steps"] = srv.steps - steps0
+                d = {k: srv.stats[k] - stats0.get(k, 0) for k in srv.stats}
+                n_st = max(1, d.get("steps", 0))
+                st["steps"] = d.get("steps", 0)
+                st["mean_rows_per_step"] = d.get("rows", 0) / n_st
+                st["mean_used_rows_per_step"] = d.get("used_rows", 0) / n_st
+                st["mean_step_interval_ms"] = (max(c.done for c in comps) - t0) * 1e3 / n_st
+                st["host_s"] = {k: round(d.get(k, 0.0), 3) for k in ("reauth_s", "step_call_s", "layout_s",
+                                                                      "finish_s")}
             row[name] = st
-        row["served_vs_plain_comparisons"] = row["served"]["comparisons_per_s"] / row["plain"]["comparisons_per_s"]
+        if "served" in row and "plain" in row:
+            row["served_vs_plain_comparisons"] = (row["served"]["comparisons_per_s"] /
+                                                  row["plain"]["comparisons_per_s"])
         sweep.append(row)
     clk.__exit__(None, None, None)
-    ok = [r for r in sweep if r["served"]["p99_ms"] < 1000]
-    okp = [r for r in sweep if r["plain"]["p99_ms"] < 1000]
+    ok = [r for r in sweep if "served" in r and r["served"]["p99_ms"] < 1000]
+    okp = [r for r in sweep if "plain" in r and r["plain"]["p99_ms"] < 1000]
     best = max(ok, key=lambda r: r["served"]["comparisons_per_s"]) if ok else None
     bestp = max(okp, key=lambda r: r["plain"]["comparisons_per_s"]) if okp else None
     result = {

@@ -143,6 +143,7 @@ class ContinuousServer:
         self.next_chunk = 0
         self.steps = 0
         self.rows_active = 0
+        self.stats = collections.Counter()  # rows and variants per step, for occupancy reports
 
     # -- placement -------------------------------------------------------------
     def n_chunks(self, db_len: int | None = None) -> int:
@@ -304,6 +305,7 @@ class ContinuousServer:
     def _finish(self, done: list) -> list:
         """Match lists of the completed requests' bitmap rows (one compaction
         launch per distinct DB snapshot), rows cleared for reuse."""
+        tf = time.perf_counter()
         by_len = collections.defaultdict(list)
         for f in done:
             for v in f.variants:
@@ -326,6 +328,7 @@ class ContinuousServer:
                 heapq.heappush(self.free_variants, v.vid)
             out.append(Completion(f.idx, f.arrival, now, res))
         self.layout_dirty = True
+        self.stats["finish_s"] += time.perf_counter() - tf
         return out
 
     def step(self) -> list:
@@ -337,7 +340,9 @@ class ContinuousServer:
         if not self.flight:
             return []
         if self.layout_dirty:
+            tl = time.perf_counter()
             self._upload_layout()
+            self.stats["layout_s"] += time.perf_counter() - tl
         k = self.next_chunk % self.n_chunks()
         off = k * self.chunk
         ln = min(self.chunk, self.db_len - off)
@@ -345,6 +350,10 @@ class ContinuousServer:
         dot_many(self.ce + self.me, MULTS, off, ln)
         self.dc.compare_threshold_open_prepared(self.c, self.ce, self.me, off, ln, self.A)
         self.steps += 1
+        self.stats["steps"] += 1
+        self.stats["rows"] += self.rows_active
+        self.stats["used_rows"] += sum(bin(x).count("1") for x in self.slot_occ)
+        self.stats["entries"] += ln
         self.next_chunk = (k + 1) % self.n_chunks()
         done, keep = [], []
         for f in self.flight:
@@ -355,11 +364,13 @@ class ContinuousServer:
         self.flight = keep
         return self._finish(done)
 
-    def serve(self, arrivals, requests, appends=None, max_wall_s: float = 600.0) -> list:
+    def serve(self, arrivals, requests, appends=None, max_wall_s: float = 600.0, lookahead: int = 256) -> list:
         """Open-loop run: request i arrives at arrivals[i] seconds after start.
         appends: {request index: (code_records, mask_records)} for requests of
-        kind "append".  Requests are taken in arrival order; one that does not
-        fit waits (with those behind it) until rows free up.  Returns the
+        kind "append".  Waiting requests are admitted in arrival order; one
+        that does not fit yet is passed by later ones that do (within
+        `lookahead` waiting requests), but never by an append, so every
+        request sees exactly the appends that arrived before it.  Returns the
         completions (latency = done - arrival)."""
         t0 = time.perf_counter()
         pending = collections.deque(sorted(range(len(requests)), key=lambda i: arrivals[i]))
@@ -373,21 +384,39 @@ class ContinuousServer:
             while pending and arrivals[pending[0]] <= now:
                 waiting.append(pending.popleft())
             reauth_items = []
-            while waiting and self.can_admit(requests[waiting[0]]):
+            kept = collections.deque()
+            barrier = False
+            scanned = 0
+            while waiting:
                 i = waiting.popleft()
                 r = requests[i]
+                if barrier or scanned >= lookahead:
+                    kept.append(i)
+                    continue
+                scanned += 1
                 if r.kind == "append":
+                    if kept:  # earlier requests still wait: the append waits behind them
+                        barrier = True
+                        kept.append(i)
+                        continue
                     code, mask = appends[i]
                     self.append(code, mask)
                     completions.append(Completion(i, t0 + arrivals[i], time.perf_counter(), Result()))
                 elif r.kind == "reauth":
                     reauth_items.append((i, t0 + arrivals[i], r))
-                else:
+                elif self.can_admit(r):
                     self.admit(r, i, t0 + arrivals[i])
+                else:
+                    kept.append(i)
+            waiting = kept
+            th = time.perf_counter()
             for start in range(0, len(reauth_items), self.max_reauth):
                 completions += self.run_reauth(reauth_items[start:start + self.max_reauth])
+            ts = time.perf_counter()
+            self.stats["reauth_s"] += ts - th
             if self.flight:
                 completions += self.step()
+                self.stats["step_call_s"] += time.perf_counter() - ts
             elif pending and not waiting:
                 time.sleep(max(0.0, min(0.002, arrivals[pending[0]] - (time.perf_counter() - t0))))
         self.dm.synchronize()

@@ -93,3 +93,73 @@ def test_split_record_i8_roundtrip():
     assert lo.dtype == np.int8 and hi.dtype == np.int8
     back = ((lo.view(np.uint8) ^ 0x80).astype(np.uint16) | ((hi.view(np.uint8) ^ 0x80).astype(np.uint16) << 8))
     assert np.array_equal(back, r)
+
+
+class _Fake:
+    """Stands in for the device objects: records calls, returns empty matches."""
+
+    def __init__(self):
+        self.calls = collections.Counter()
+
+    def __getattr__(self, name):
+        def f(*a, **k):
+            self.calls[name] += 1
+        return f
+
+
+class _FakeDC(_Fake):
+    def take_rows(self, rows, db_len, clear=True):
+        self.calls["take_rows"] += 1
+        return np.zeros(len(rows), np.uint32), np.zeros((len(rows), 256), np.uint32)
+
+
+def _fake_server(monkeypatch, db_len=1000, chunk=256, rows=128, max_variants=16):
+    import irisb200.serving as S
+    monkeypatch.setattr(S, "dot_many", lambda *a, **k: None)
+    s = ContinuousServer.__new__(ContinuousServer)
+    s.dm, s.c = _Fake(), _Fake()
+    s.ce, s.me = [_Fake() for _ in range(3)], [_Fake() for _ in range(3)]
+    s.dc = _FakeDC()
+    s.A, s.chunk = 16384, chunk
+    s.row_capacity = rows
+    s.n_slot_cap = rows // 32
+    s.slot_occ = [0] * s.n_slot_cap
+    s.slot_vars = [[] for _ in range(s.n_slot_cap)]
+    s.max_variants = max_variants
+    s.db_len, s.db_capacity = db_len, db_len + 10
+    s.free_variants = list(range(max_variants))
+    s.pending_bases = {}
+    s.max_reauth = 4
+    s.flight, s.layout_dirty, s.next_chunk, s.steps, s.rows_active = [], False, 0, 0, 0
+    s.stats = collections.Counter()
+    appended = []
+    s.append = lambda code, mask: appended.append(s.db_len) or setattr(s, "db_len", s.db_len + 1)
+    s.run_reauth = lambda items: [S.Completion(i, a, a, S.Result(reauth_match=False)) for i, a, _ in items]
+    return s, appended
+
+
+def test_serve_loop_admission_and_append_barrier(monkeypatch):
+    from irisb200.batched import Request
+    s, appended = _fake_server(monkeypatch)
+    zc, zm = np.zeros((3, 12800), np.uint16), np.zeros((3, 6400), np.uint16)
+    reqs = [Request(code=zc, mask=zm, n_rot=31, mirrored=True) for _ in range(3)]        # 2 words each
+    reqs += [Request(code=zc, mask=zm, n_rot=1), Request(code=None, mask=None, kind="append"),
+             Request(code=zc, mask=zm, n_rot=1), Request(code=zc, mask=zm, kind="reauth", target=3)]
+    admitted_at = {}
+    orig_admit = ContinuousServer.admit
+
+    def admit(self, r, idx, arrival):
+        admitted_at[idx] = (self.steps, self.db_len)
+        return orig_admit(self, r, idx, arrival)
+    monkeypatch.setattr(ContinuousServer, "admit", admit)
+    comps = s.serve([0.0] * len(reqs), reqs, appends={4: (None, None)})
+    assert sorted(c.idx for c in comps) == list(range(len(reqs)))
+    # 4 words: requests 0 and 1 fit, 2 waits; the 1-row request 3 passes it (bypass) ...
+    assert admitted_at[0][0] == 0 and admitted_at[1][0] == 0 and admitted_at[3][0] == 0
+    assert admitted_at[2][0] > 0
+    # ... but the append waits behind request 2, and request 5 behind the append
+    assert appended == [1000]
+    assert admitted_at[2][1] == 1000 and admitted_at[5][1] == 1001
+    # every uniqueness request visited all 4 chunks of its DB snapshot
+    assert s.steps >= 8 and not s.flight and sorted(s.free_variants) == list(range(16))
+    assert s.slot_occ == [0, 0, 0, 0]
