@@ -611,8 +611,7 @@ def run_serving(args):
                 st["mean_rows_per_step"] = d.get("rows", 0) / n_st
                 st["mean_used_rows_per_step"] = d.get("used_rows", 0) / n_st
                 st["mean_step_interval_ms"] = (max(c.done for c in comps) - t0) * 1e3 / n_st
-                st["host_s"] = {k: round(d.get(k, 0.0), 3) for k in ("reauth_s", "step_call_s", "layout_s",
-                                                                      "finish_s")}
+                st["host_s"] = {k: round(d.get(k, 0.0), 3) for k in ("launch_s", "layout_s", "wait_s")}
             row[name] = st
         if "served" in row and "plain" in row:
             row["served_vs_plain_comparisons"] = (row["served"]["comparisons_per_s"] /

@@ -76,6 +76,23 @@ int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_
 int irs_device_manager_advance_batch_counter(irs_device_manager* dm, void* stream);
 /* Number of SMs the persistent kernels size their grids to. */
 int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
+/* Host synchronisation of the calls that take host buffers (default on).
+ * With it off, irs_sharedb_query_put_base, irs_sharedb_query_expand_rows,
+ * irs_sharedb_query_upload_rows, irs_sharedb_gather_records,
+ * irs_dc_set_segments and irs_dc_take_rows return as soon as their copies and
+ * kernels are enqueued: their host buffers must then be page-locked
+ * (irs_host_alloc_pinned) and stay unchanged until the work has run, and
+ * take_rows outputs are valid after an event recorded behind them on the
+ * party-0 stream has completed (device errors: irs_device_manager_error).  A
+ * serving loop uses this to prepare and launch step k+1 while step k runs. */
+int irs_device_manager_set_host_sync(irs_device_manager* dm, int on);
+/* CUDA events for the asynchronous mode (cudaEventDisableTiming). */
+int irs_event_create(void** ev);
+int irs_event_record(void* ev, void* stream);
+int irs_event_synchronize(void* ev);
+/* *done = 1 when the work before the event has completed, else 0. */
+int irs_event_query(void* ev, int* done);
+int irs_event_destroy(void* ev);
 /* Free and total device memory (cudaMemGetInfo), for admission by free HBM. */
 int irs_device_manager_mem_info(irs_device_manager* dm, size_t* free_bytes, size_t* total_bytes);
 

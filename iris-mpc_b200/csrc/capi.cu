@@ -62,6 +62,7 @@ struct irs_device_manager {
   uint64_t* d_batch = nullptr;  // device batch counter (irs_device_manager_set_batch_counter)
   bool capturing = false;  // a graph capture on streams[0] is open
   cudaEvent_t graph_done = nullptr;  // recorded after each graph launch
+  bool host_sync = true;  // false: host-buffer calls return once enqueued (irs_device_manager_set_host_sync)
 };
 
 struct irs_graph {
@@ -306,6 +307,49 @@ int irs_sharedb_use_batch_counter(irs_sharedb* db, int on) {
 int irs_circuits_use_batch_counter(irs_circuits* c, int on) {
   CHECK(c, IRS_ERR_INVALID, "c is NULL");
   c->batch_from_device = on != 0;
+  return IRS_OK;
+}
+
+int irs_device_manager_set_host_sync(irs_device_manager* dm, int on) {
+  CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
+  dm->host_sync = on != 0;
+  return IRS_OK;
+}
+
+int irs_event_create(void** ev) {
+  CHECK(ev, IRS_ERR_INVALID, "ev is NULL");
+  cudaEvent_t e = nullptr;
+  CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  *ev = e;
+  return IRS_OK;
+}
+
+int irs_event_record(void* ev, void* stream) {
+  CHECK(ev, IRS_ERR_INVALID, "ev is NULL");
+  CU(cudaEventRecord(static_cast<cudaEvent_t>(ev), static_cast<cudaStream_t>(stream)));
+  return IRS_OK;
+}
+
+int irs_event_synchronize(void* ev) {
+  CHECK(ev, IRS_ERR_INVALID, "ev is NULL");
+  CU(cudaEventSynchronize(static_cast<cudaEvent_t>(ev)));
+  return IRS_OK;
+}
+
+int irs_event_query(void* ev, int* done) {
+  CHECK(ev && done, IRS_ERR_INVALID, "bad arguments");
+  const cudaError_t e = cudaEventQuery(static_cast<cudaEvent_t>(ev));
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return IRS_OK;
+  }
+  CU(e);
+  *done = 1;
+  return IRS_OK;
+}
+
+int irs_event_destroy(void* ev) {
+  if (ev) cudaEventDestroy(static_cast<cudaEvent_t>(ev));
   return IRS_OK;
 }
 
@@ -638,7 +682,7 @@ int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t 
   CU(cudaMemcpyAsync(stage + table_off, row_desc, table_bytes, cudaMemcpyHostToDevice, s));
   CU(launch_expand_rows(db->q_stage, (uint32_t)K, reinterpret_cast<const uint32_t*>(stage + table_off), (uint32_t)n_rows,
                         (uint32_t)db->n_pad, db->q_lo, db->q_hi, s));
-  CU(cudaStreamSynchronize(s));  // base / row_desc are caller-owned host memory
+  if (dm->host_sync) CU(cudaStreamSynchronize(s));  // base / row_desc are caller-owned host memory
   db->have_query = true;
   return IRS_OK;
 }
@@ -653,7 +697,7 @@ int irs_sharedb_query_put_base(irs_sharedb* db, size_t first, size_t n, const ui
   cudaStream_t s = dm->streams[db->peer];
   if (n) {
     CU(cudaMemcpyAsync(db->q_stage + first * K, base, n * K * 2, cudaMemcpyHostToDevice, s));
-    CU(cudaStreamSynchronize(s));  // caller-owned host memory
+    if (dm->host_sync) CU(cudaStreamSynchronize(s));  // caller-owned host memory
   }
   return IRS_OK;
 }
@@ -678,7 +722,7 @@ int irs_sharedb_query_expand_rows(irs_sharedb* db, size_t n_base, const uint32_t
   CU(cudaMemcpyAsync(stage + table_off, row_desc, table_bytes, cudaMemcpyHostToDevice, s));
   CU(launch_expand_rows(db->q_stage, (uint32_t)K, reinterpret_cast<const uint32_t*>(stage + table_off), (uint32_t)n_rows,
                         (uint32_t)db->n_pad, db->q_lo, db->q_hi, s));
-  CU(cudaStreamSynchronize(s));  // row_desc is caller-owned host memory
+  if (dm->host_sync) CU(cudaStreamSynchronize(s));  // row_desc is caller-owned host memory
   db->have_query = true;
   return IRS_OK;
 }
@@ -701,7 +745,7 @@ int irs_sharedb_gather_records(irs_sharedb* dst, irs_sharedb* src, const uint32_
   CU(cudaMemcpyAsync(dst->q_stage, ids, n * 4, cudaMemcpyHostToDevice, s));
   CU(launch_gather_rows(src->db_lo, src->db_hi, reinterpret_cast<const uint32_t*>(dst->q_stage), (uint32_t)n,
                         (uint32_t)K, dst->db_lo, dst->db_hi, s));
-  CU(cudaStreamSynchronize(s));
+  if (dm->host_sync) CU(cudaStreamSynchronize(s));  // ids is caller-owned host memory
   dst->db_len = n;
   return IRS_OK;
 }
@@ -1102,7 +1146,7 @@ int irs_dc_set_segments(irs_distance_comparator* dc, size_t n_slots, const uint3
     CU(cudaMemcpyAsync(dc->d_seg_query, seg_query, n_seg * 4, cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(dc->d_seg_mask, seg_mask, n_seg * 4, cudaMemcpyHostToDevice, s));
   }
-  CU(cudaStreamSynchronize(s));
+  if (dm->host_sync) CU(cudaStreamSynchronize(s));  // the tables are caller-owned host memory
   dc->n_seg_slots = n_slots;
   dc->have_segments = true;
   return IRS_OK;
@@ -1230,6 +1274,7 @@ int irs_dc_take_rows(irs_distance_comparator* dc, const uint32_t* rows, size_t n
                       d_counts, d_ids, kMaxMatchesLen, s));
   CU(cudaMemcpyAsync(counts, d_counts, n * 4, cudaMemcpyDeviceToHost, s));
   CU(cudaMemcpyAsync(ids, d_ids, n * kMaxMatchesLen * 4, cudaMemcpyDeviceToHost, s));
+  if (!dm->host_sync) return IRS_OK;  // outputs valid once the stream passes the copies
   CU(cudaStreamSynchronize(s));
   return check_device_error(dm);
 }

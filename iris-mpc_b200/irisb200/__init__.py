@@ -58,6 +58,12 @@ _SIGS = {
     "irs_device_manager_clear_error": [_vp],
     "irs_device_manager_sm_count": [_vp, C.POINTER(_i)],
     "irs_device_manager_mem_info": [_vp, C.POINTER(_sz), C.POINTER(_sz)],
+    "irs_device_manager_set_host_sync": [_vp, _i],
+    "irs_event_create": [C.POINTER(_vp)],
+    "irs_event_record": [_vp, _vp],
+    "irs_event_synchronize": [_vp],
+    "irs_event_query": [_vp, C.POINTER(_i)],
+    "irs_event_destroy": [_vp],
     "irs_dc_clear_rows": [_vp, _sz, _sz, _vp],
     "irs_dc_take_rows": [_vp, _vp, _sz, _sz, _i, _vp, _vp],
     "irs_dc_fetch_rows": [_vp, _sz, _sz, _vp, _sz, C.POINTER(_sz)],
@@ -282,6 +288,31 @@ def synth_queries(db_seed: int, q_seed: int, n_queries: int, planted: dict, prep
     return code, mask
 
 
+class Event:
+    """A CUDA event (no timing) for the asynchronous host mode."""
+
+    def __init__(self):
+        p = _vp()
+        _check(lib().irs_event_create(C.byref(p)))
+        self.h = p.value
+
+    def record(self, stream=None) -> None:
+        _check(lib().irs_event_record(self.h, stream))
+
+    def synchronize(self) -> None:
+        _check(lib().irs_event_synchronize(self.h))
+
+    def done(self) -> bool:
+        d = _i()
+        _check(lib().irs_event_query(self.h, C.byref(d)))
+        return bool(d.value)
+
+    def close(self) -> None:
+        if self.h:
+            lib().irs_event_destroy(self.h)
+            self.h = None
+
+
 class DeviceManager:
     """DeviceManager (iris-mpc-gpu/src/helpers/device_manager.rs) for one GPU
     hosting the three parties, each with its own stream and memory pool."""
@@ -310,6 +341,10 @@ class DeviceManager:
 
     def advance_batch_counter(self, stream=None) -> None:
         _check(lib().irs_device_manager_advance_batch_counter(self.h, stream))
+
+    def set_host_sync(self, on: bool) -> None:
+        """See irs_device_manager_set_host_sync: off = enqueue-only calls on pinned host buffers."""
+        _check(lib().irs_device_manager_set_host_sync(self.h, int(on)))
 
     def mem_info(self):
         f, t = _sz(), _sz()
@@ -530,6 +565,17 @@ class DistanceComparator:
         _check(lib().irs_dc_take_rows(self.h, _ptr(r) if r.size else None, r.size, db_len, int(clear), _ptr(counts),
                                       _ptr(ids)))
         return counts[: r.size], ids[: r.size]
+
+    def take_rows_into(self, rows: np.ndarray, db_len: int, counts: np.ndarray, ids: np.ndarray,
+                       clear: bool = True) -> None:
+        """irs_dc_take_rows into caller-owned arrays (page-locked, and read only
+        after the stream has passed the call, in the asynchronous host mode)."""
+        for a, dt in ((rows, np.uint32), (counts, np.uint32), (ids, np.uint32)):
+            if a.dtype != dt or not a.flags.c_contiguous:
+                raise ValueError("take_rows_into needs contiguous uint32 arrays")
+        if counts.size < rows.size or ids.shape[0] < rows.size or ids.shape[1] != MAX_MATCHES_LEN:
+            raise ValueError("output arrays too small")
+        _check(lib().irs_dc_take_rows(self.h, _ptr(rows), rows.size, db_len, int(clear), _ptr(counts), _ptr(ids)))
 
     def clear_rows(self, first: int, n: int, stream=None) -> None:
         _check(lib().irs_dc_clear_rows(self.h, first, n, stream))

@@ -35,7 +35,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import IRIS_CODE_LENGTH, MASK_CODE_LENGTH, DistanceComparator, ShareDB, dot_many, mirror_query_share
+from . import (IRIS_CODE_LENGTH, MASK_CODE_LENGTH, MAX_MATCHES_LEN, DistanceComparator, Event, IrisError,
+               PinnedArray, ShareDB, dot_many, mirror_query_share)
 from .batched import MULTS, Request, Result, centred_rotations, pack
 
 RESULT_BYTES_PER_ROW_ENTRY = 2 * 6  # u16 dot share per (row, entry) for 6 engines
@@ -103,7 +104,13 @@ class ContinuousServer:
     at code_engines[p], mask at mask_engines[p]).  The engines hold the DB
     (alloc_db with room for appends) and must be created with max_db_length
     >= chunk (result rows) and query_length >= row_capacity, with row_capacity
-    above max_variants (the base pool shares the query staging)."""
+    above max_variants (the base pool shares the query staging).
+
+    serve() runs the device work one step ahead of the host: step k+1 (its
+    uploads, GEMMs, threshold and the match-list compaction of the requests
+    that finish with it) is enqueued before the host waits for step k's
+    results, with the library in its asynchronous host mode and every host
+    buffer it reads or writes page-locked and double-buffered."""
 
     def __init__(self, dm, code_engines, mask_engines, circuits, chunk: int = 65536, row_capacity: int = 2048,
                  max_variants: int = 512, max_reauth: int = 64, threshold_a: int = 16384, seeds=None,
@@ -125,7 +132,7 @@ class ContinuousServer:
         self.dc = DistanceComparator(dm, max_variants, max(self.db_capacity, 64), match_list_cap=1 << 16)
         self.dc.reset()
         self.free_variants = list(range(max_variants))  # min-heap: low ids keep pool writes contiguous
-        self.pending_bases = {}  # vid -> (code [3][12800], mask [3][6400]) not yet in the device pool
+        self.pending_bases = set()  # pool indices written on the host, not yet copied to the device pool
         seeds = seeds or [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
         self.max_reauth = max_reauth
         nsub = 2 * max_reauth
@@ -138,12 +145,41 @@ class ContinuousServer:
             e.use_batch_counter(True)
         circuits.use_batch_counter(True)
         dm.set_batch_counter(1)
+        self._alloc_host(nsub)
         self.flight = []
         self.layout_dirty = False
         self.next_chunk = 0
         self.steps = 0
         self.rows_active = 0
         self.stats = collections.Counter()  # rows and variants per step, for occupancy reports
+
+    def _alloc_host(self, nsub: int) -> None:
+        """Page-locked host buffers: the base-query pool mirror (one slot per
+        pool index, written once per admission) and two sets (one per step in
+        flight) of row tables, segment tables, compaction outputs and reauth
+        staging."""
+        V, R = self.max_variants, self.row_capacity
+        P = PinnedArray
+        self.h_pool_c = P((3, V, IRIS_CODE_LENGTH), np.uint16)
+        self.h_pool_m = P((3, V, MASK_CODE_LENGTH), np.uint16)
+        self.h_rows = [P((R,), np.uint32) for _ in range(2)]
+        self.h_seg = [(P((self.n_slot_cap + 1,), np.uint32), P((R,), np.uint32), P((R,), np.uint32))
+                      for _ in range(2)]
+        self.h_take = [(P((V,), np.uint32), P((V,), np.uint32), P((V, MAX_MATCHES_LEN), np.uint32))
+                       for _ in range(2)]
+        self.h_r_ids = [P((nsub,), np.uint32) for _ in range(2)]
+        self.h_r_base = [(P((3, nsub, IRIS_CODE_LENGTH), np.uint16), P((3, nsub, MASK_CODE_LENGTH), np.uint16))
+                         for _ in range(2)]
+        self.h_r_rows = [P((nsub * 32,), np.uint32) for _ in range(2)]
+        self.h_r_seg = [(P((nsub + 1,), np.uint32), P((nsub * 32,), np.uint32), P((nsub * 32,), np.uint32))
+                        for _ in range(2)]
+        self.h_r_take = [(P((nsub,), np.uint32), P((nsub,), np.uint32), P((nsub, MAX_MATCHES_LEN), np.uint32))
+                         for _ in range(2)]
+        self.events = [Event(), Event()]
+        self.par = 0
+        # pool indices of completed variants, reusable once their step's event has
+        # completed (a pinned pool slot may still be read by a queued copy before)
+        self.cooling = [[], []]
 
     # -- placement -------------------------------------------------------------
     def n_chunks(self, db_len: int | None = None) -> int:
@@ -190,7 +226,8 @@ class ContinuousServer:
 
     def admit(self, r: Request, idx: int, arrival: float) -> None:
         """Places the request's variants and writes their base shares into
-        the resident pool (pool index = bitmap row)."""
+        the host mirror of the pool (pool index = bitmap row); the next step
+        copies them to the device."""
         variants = []
         for mir in ([False, True] if r.mirrored else [False]):
             where = self._place(r.n_rot)
@@ -199,9 +236,10 @@ class ContinuousServer:
             v = _Variant(heapq.heappop(self.free_variants), mir, list(centred_rotations(r.n_rot)))
             self._occupy(v, *where)
             variants.append(v)
-            code = np.stack([mirror_query_share(r.code[p], True) if mir else r.code[p] for p in range(3)])
-            mask = np.stack([mirror_query_share(r.mask[p], False) if mir else r.mask[p] for p in range(3)])
-            self.pending_bases[v.vid] = (code, mask)
+            for p in range(3):
+                self.h_pool_c.array[p, v.vid] = mirror_query_share(r.code[p], True) if mir else r.code[p]
+                self.h_pool_m.array[p, v.vid] = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
+            self.pending_bases.add(v.vid)
         f = _Flight(r, idx, arrival, self.db_len, variants, set(range(math.ceil(self.db_len / self.chunk))))
         self.flight.append(f)
         self.layout_dirty = True
@@ -222,28 +260,32 @@ class ContinuousServer:
         return row_desc, np.array(seg_start, np.uint32), np.array(seg_query, np.uint32), np.array(seg_mask, np.uint32)
 
     def _flush_bases(self) -> None:
-        """Writes the newly admitted variants' base shares into the device
-        pool, one copy per engine per contiguous run of pool indices."""
+        """Copies the newly admitted variants' base shares from the pinned
+        host pool into the device pool, one copy per engine per contiguous
+        run of pool indices."""
         vids = sorted(self.pending_bases)
-        runs, start = [], 0
+        start = 0
         for i in range(1, len(vids) + 1):
             if i == len(vids) or vids[i] != vids[i - 1] + 1:
-                runs.append(vids[start:i])
+                a, n = vids[start], i - start
+                for p in range(3):
+                    self.ce[p].query_put_base(a, self.h_pool_c.array[p, a:a + n])
+                    self.me[p].query_put_base(a, self.h_pool_m.array[p, a:a + n])
                 start = i
-        for run in runs:
-            code = np.stack([self.pending_bases[v][0] for v in run], axis=1)  # [3][n][12800]
-            mask = np.stack([self.pending_bases[v][1] for v in run], axis=1)
-            for p in range(3):
-                self.ce[p].query_put_base(run[0], code[p])
-                self.me[p].query_put_base(run[0], mask[p])
         self.pending_bases.clear()
 
     def _upload_layout(self) -> None:
         self._flush_bases()
         row_desc, seg_start, seg_query, seg_mask = self._layout()
+        rt = self.h_rows[self.par].array[: row_desc.size]
+        rt[:] = row_desc
+        ss, sq, sm = (x.array for x in self.h_seg[self.par])
+        ss[: seg_start.size] = seg_start
+        sq[: seg_query.size] = seg_query
+        sm[: seg_mask.size] = seg_mask
         for e in self.ce + self.me:
-            e.query_expand_rows(self.max_variants, row_desc)
-        self.dc.set_segments(seg_start, seg_query, seg_mask)
+            e.query_expand_rows(self.max_variants, rt)
+        self.dc.set_segments(ss[: seg_start.size], sq[: seg_query.size], sm[: seg_mask.size])
         self.rows_active = row_desc.size
         self.layout_dirty = False
 
@@ -262,107 +304,147 @@ class ContinuousServer:
         self.db_len = idx + 1
         return idx
 
-    def run_reauth(self, items) -> list:
-        """items: [(idx, arrival, Request)] -> [Completion]."""
+    def _launch_reauth(self, items):
+        """Enqueues one reauth batch (items: [(idx, arrival, Request)]) on the
+        gathered subset; returns the handler that turns its compacted rows
+        into completions once the step's event has completed."""
         for _, _, r in items:
             if not 0 <= r.target < self.db_len:
                 raise ValueError(f"reauth target {r.target} is not in the DB")
+        par = self.par
         variants = [(j, False) for j in range(len(items))] + \
                    [(j, True) for j, (_, _, r) in enumerate(items) if r.mirrored]
-        ids = np.array([items[j][2].target for j, _ in variants], np.uint32)
+        n = len(variants)
+        ids = self.h_r_ids[par].array[:n]
+        ids[:] = [items[j][2].target for j, _ in variants]
         for p in range(3):
             self.sce[p].gather_records(self.ce[p], ids)
             self.sme[p].gather_records(self.me[p], ids)
         layout = pack([list(centred_rotations(items[j][2].n_rot)) for j, _ in variants])
-        bc = np.zeros((3, len(variants), IRIS_CODE_LENGTH), np.uint16)
-        bm = np.zeros((3, len(variants), MASK_CODE_LENGTH), np.uint16)
+        bc, bm = (x.array for x in self.h_r_base[par])
         for v, (j, mir) in enumerate(variants):
             r = items[j][2]
             for p in range(3):
                 bc[p, v] = mirror_query_share(r.code[p], True) if mir else r.code[p]
                 bm[p, v] = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
+        rt = self.h_r_rows[par].array[: layout.n_rows]
+        rt[:] = layout.row_desc
         for p in range(3):
-            self.sce[p].query_upload_rows(bc[p], layout.row_desc)
-            self.sme[p].query_upload_rows(bm[p], layout.row_desc)
+            self.sce[p].query_upload_rows(bc[p, :n], rt)
+            self.sme[p].query_upload_rows(bm[p, :n], rt)
+        ss, sq, sm = (x.array for x in self.h_r_seg[par])
+        ns, nq = layout.seg_start.size, layout.seg_query.size
+        ss[:ns], sq[:nq], sm[:nq] = layout.seg_start, layout.seg_query, layout.seg_mask
         self.dm.advance_batch_counter()
-        n = len(variants)
         self.sdc.reset()
-        self.sdc.set_segments(layout.seg_start, layout.seg_query, layout.seg_mask)
+        self.sdc.set_segments(ss[:ns], sq[:nq], sm[:nq])
         dot_many(self.sce + self.sme, MULTS, 0, n)
         self.sdc.compare_threshold_open_prepared(self.c, self.sce, self.sme, 0, n, self.A)
-        rows = self.sdc.fetch_rows(0, n, n)
-        now = time.perf_counter()
-        out = {j: Result() for j in range(len(items))}
-        for v, (j, mir) in enumerate(variants):
-            hit = bool(rows[v, v])  # variant v against its own target (subset record v)
-            if mir:
-                out[j].reauth_mirror_match = hit
-            else:
-                out[j].reauth_match = hit
-        return [Completion(items[j][0], items[j][1], now, out[j]) for j in range(len(items))]
+        rows, counts, tids = (x.array for x in self.h_r_take[par])
+        rows[:n] = np.arange(n, dtype=np.uint32)
+        self.sdc.take_rows_into(rows[:n], n, counts, tids, clear=True)
+
+        def handler(now):
+            out = {j: Result() for j in range(len(items))}
+            for v, (j, mir) in enumerate(variants):
+                hit = v in tids[v, : min(int(counts[v]), MAX_MATCHES_LEN)]  # against its own target (record v)
+                if mir:
+                    out[j].reauth_mirror_match = bool(hit)
+                else:
+                    out[j].reauth_match = bool(hit)
+            return [Completion(items[j][0], items[j][1], now, out[j]) for j in range(len(items))]
+        return handler
 
     # -- the chunk step -------------------------------------------------------------
-    def _finish(self, done: list) -> list:
-        """Match lists of the completed requests' bitmap rows (one compaction
-        launch per distinct DB snapshot), rows cleared for reuse."""
-        tf = time.perf_counter()
+    def _launch_step(self):
+        """Enqueues one DB chunk for every request in flight and the match
+        compaction of the requests it completes (their rows are released on
+        the host at once: every later use of those rows is ordered after the
+        compaction on the device).  Returns the completion handler or None."""
+        empty = [f for f in self.flight if not f.needed]  # admitted against an empty DB
+        if not self.flight:
+            return None
+        done = list(empty)
+        keep = [f for f in self.flight if f.needed]
+        if keep:
+            if self.layout_dirty:
+                tl = time.perf_counter()
+                self._upload_layout()
+                self.stats["layout_s"] += time.perf_counter() - tl
+            k = self.next_chunk % self.n_chunks()
+            off = k * self.chunk
+            ln = min(self.chunk, self.db_len - off)
+            self.dm.advance_batch_counter()
+            dot_many(self.ce + self.me, MULTS, off, ln)
+            self.dc.compare_threshold_open_prepared(self.c, self.ce, self.me, off, ln, self.A)
+            self.steps += 1
+            self.stats["steps"] += 1
+            self.stats["rows"] += self.rows_active
+            self.stats["used_rows"] += sum(bin(x).count("1") for x in self.slot_occ)
+            self.stats["entries"] += ln
+            self.next_chunk = (k + 1) % self.n_chunks()
+            still = []
+            for f in keep:
+                f.needed.discard(k)
+                (still if f.needed else done).append(f)
+            keep = still
+        self.flight = keep
+        if not done:
+            return None
+        rows, counts, ids = (x.array for x in self.h_take[self.par])
         by_len = collections.defaultdict(list)
         for f in done:
             for v in f.variants:
                 by_len[f.db_len].append(v)
-        hits = {}
+        where, off = {}, 0
         for db_len, vs in by_len.items():
-            counts, ids = self.dc.take_rows([v.vid for v in vs], db_len, clear=True)
-            for v, n, row in zip(vs, counts, ids):
-                hits[v.vid] = row[: min(int(n), len(row))].tolist()
+            n = len(vs)
+            rows[off:off + n] = [v.vid for v in vs]
+            if db_len:
+                self.dc.take_rows_into(rows[off:off + n], db_len, counts[off:off + n], ids[off:off + n],
+                                       clear=True)
+            else:
+                counts[off:off + n] = 0
+            for i, v in enumerate(vs):
+                where[v.vid] = off + i
+            off += n
+        for f in done:
+            for v in f.variants:
+                self._release(v)
+                self.cooling[self.par].append(v.vid)
+        self.layout_dirty = True
+
+        def handler(now):
+            out = []
+            for f in done:
+                res = Result()
+                for v in f.variants:
+                    i = where[v.vid]
+                    hits = ids[i, : min(int(counts[i]), MAX_MATCHES_LEN)].tolist()
+                    if v.mirrored:
+                        res.mirror_matches = hits
+                    else:
+                        res.matches = hits
+                out.append(Completion(f.idx, f.arrival, now, res))
+            return out
+        return handler
+
+    def _collect(self, pending) -> list:
+        ev, handlers, par = pending
+        tw = time.perf_counter()
+        ev.synchronize()
+        self.stats["wait_s"] += time.perf_counter() - tw
+        for vid in self.cooling[par]:
+            heapq.heappush(self.free_variants, vid)
+        self.cooling[par].clear()
+        code = self.dm.error_code()
+        if code:
+            raise IrisError(code, "a kernel reported a device error during serving")
         now = time.perf_counter()
         out = []
-        for f in done:
-            res = Result()
-            for v in f.variants:
-                if v.mirrored:
-                    res.mirror_matches = hits[v.vid]
-                else:
-                    res.matches = hits[v.vid]
-                self._release(v)
-                heapq.heappush(self.free_variants, v.vid)
-            out.append(Completion(f.idx, f.arrival, now, res))
-        self.layout_dirty = True
-        self.stats["finish_s"] += time.perf_counter() - tf
+        for h in handlers:
+            out += h(now)
         return out
-
-    def step(self) -> list:
-        """One DB chunk for every request in flight; returns completions."""
-        empty = [f for f in self.flight if not f.needed]
-        if empty:  # admitted against an empty DB
-            self.flight = [f for f in self.flight if f.needed]
-            return self._finish(empty)
-        if not self.flight:
-            return []
-        if self.layout_dirty:
-            tl = time.perf_counter()
-            self._upload_layout()
-            self.stats["layout_s"] += time.perf_counter() - tl
-        k = self.next_chunk % self.n_chunks()
-        off = k * self.chunk
-        ln = min(self.chunk, self.db_len - off)
-        self.dm.advance_batch_counter()
-        dot_many(self.ce + self.me, MULTS, off, ln)
-        self.dc.compare_threshold_open_prepared(self.c, self.ce, self.me, off, ln, self.A)
-        self.steps += 1
-        self.stats["steps"] += 1
-        self.stats["rows"] += self.rows_active
-        self.stats["used_rows"] += sum(bin(x).count("1") for x in self.slot_occ)
-        self.stats["entries"] += ln
-        self.next_chunk = (k + 1) % self.n_chunks()
-        done, keep = [], []
-        for f in self.flight:
-            f.needed.discard(k)
-            (keep if f.needed else done).append(f)
-        if not done:
-            return []
-        self.flight = keep
-        return self._finish(done)
 
     def serve(self, arrivals, requests, appends=None, max_wall_s: float = 600.0, lookahead: int = 256) -> list:
         """Open-loop run: request i arrives at arrivals[i] seconds after start.
@@ -373,58 +455,76 @@ class ContinuousServer:
         request sees exactly the appends that arrived before it.  Returns the
         completions (latency = done - arrival)."""
         t0 = time.perf_counter()
-        pending = collections.deque(sorted(range(len(requests)), key=lambda i: arrivals[i]))
+        order = collections.deque(sorted(range(len(requests)), key=lambda i: arrivals[i]))
         waiting = collections.deque()
         completions = []
         total = len(requests)
-        while len(completions) < total:
-            now = time.perf_counter() - t0
-            if now > max_wall_s:
-                raise TimeoutError("serving run exceeded its wall-clock budget")
-            while pending and arrivals[pending[0]] <= now:
-                waiting.append(pending.popleft())
-            reauth_items = []
-            kept = collections.deque()
-            barrier = False
-            scanned = 0
-            while waiting:
-                i = waiting.popleft()
-                r = requests[i]
-                if barrier or scanned >= lookahead:
-                    kept.append(i)
-                    continue
-                scanned += 1
-                if r.kind == "append":
-                    if kept:  # earlier requests still wait: the append waits behind them
-                        barrier = True
+        pending = None  # (event, handlers) of the step in flight
+        self.dm.set_host_sync(False)
+        try:
+            while len(completions) < total:
+                now = time.perf_counter() - t0
+                if now > max_wall_s:
+                    raise TimeoutError("serving run exceeded its wall-clock budget")
+                while order and arrivals[order[0]] <= now:
+                    waiting.append(order.popleft())
+                reauth_items = []
+                kept = collections.deque()
+                barrier = False
+                scanned = 0
+                while waiting:
+                    i = waiting.popleft()
+                    r = requests[i]
+                    if barrier or scanned >= lookahead:
                         kept.append(i)
                         continue
-                    code, mask = appends[i]
-                    self.append(code, mask)
-                    completions.append(Completion(i, t0 + arrivals[i], time.perf_counter(), Result()))
-                elif r.kind == "reauth":
-                    reauth_items.append((i, t0 + arrivals[i], r))
-                elif self.can_admit(r):
-                    self.admit(r, i, t0 + arrivals[i])
-                else:
-                    kept.append(i)
-            waiting = kept
-            th = time.perf_counter()
-            for start in range(0, len(reauth_items), self.max_reauth):
-                completions += self.run_reauth(reauth_items[start:start + self.max_reauth])
-            ts = time.perf_counter()
-            self.stats["reauth_s"] += ts - th
-            if self.flight:
-                completions += self.step()
-                self.stats["step_call_s"] += time.perf_counter() - ts
-            elif pending and not waiting:
-                time.sleep(max(0.0, min(0.002, arrivals[pending[0]] - (time.perf_counter() - t0))))
-        self.dm.synchronize()
+                    scanned += 1
+                    if r.kind == "append":
+                        if kept:  # earlier requests still wait: the append waits behind them
+                            barrier = True
+                            kept.append(i)
+                            continue
+                        code, mask = appends[i]
+                        self.append(code, mask)
+                        completions.append(Completion(i, t0 + arrivals[i], time.perf_counter(), Result()))
+                    elif r.kind == "reauth" and len(reauth_items) < self.max_reauth:
+                        reauth_items.append((i, t0 + arrivals[i], r))
+                    elif r.kind == "uniqueness" and self.can_admit(r):
+                        self.admit(r, i, t0 + arrivals[i])
+                    else:
+                        kept.append(i)
+                waiting = kept
+                ts = time.perf_counter()
+                handlers = []
+                if reauth_items:
+                    handlers.append(self._launch_reauth(reauth_items))
+                h = self._launch_step()
+                if h:
+                    handlers.append(h)
+                launched = None
+                if handlers:
+                    ev = self.events[self.par]
+                    ev.record(self.dm.stream(0))
+                    launched = (ev, handlers, self.par)
+                    self.par ^= 1
+                self.stats["launch_s"] += time.perf_counter() - ts
+                if pending:
+                    completions += self._collect(pending)
+                pending = launched
+                if pending is None and not self.flight and order and not waiting:
+                    time.sleep(max(0.0, min(0.002, arrivals[order[0]] - (time.perf_counter() - t0))))
+            if pending:
+                completions += self._collect(pending)
+        finally:
+            self.dm.synchronize()
+            self.dm.set_host_sync(True)
         return completions
 
     def close(self) -> None:
         for o in self.sce + self.sme + [self.dc, self.sdc]:
             o.close()
+        for e in self.events:
+            e.close()
 
 
 class PlainBatchServer:

@@ -108,9 +108,14 @@ class _Fake:
 
 
 class _FakeDC(_Fake):
-    def take_rows(self, rows, db_len, clear=True):
+    def take_rows_into(self, rows, db_len, counts, ids, clear=True):
         self.calls["take_rows"] += 1
-        return np.zeros(len(rows), np.uint32), np.zeros((len(rows), 256), np.uint32)
+        counts[: rows.size] = 0
+
+
+class _Buf:
+    def __init__(self, shape, dtype):
+        self.array = np.zeros(shape, dtype)
 
 
 def _fake_server(monkeypatch, db_len=1000, chunk=256, rows=128, max_variants=16):
@@ -128,13 +133,17 @@ def _fake_server(monkeypatch, db_len=1000, chunk=256, rows=128, max_variants=16)
     s.max_variants = max_variants
     s.db_len, s.db_capacity = db_len, db_len + 10
     s.free_variants = list(range(max_variants))
-    s.pending_bases = {}
+    s.pending_bases = set()
     s.max_reauth = 4
+    monkeypatch.setattr(S, "PinnedArray", _Buf)
+    monkeypatch.setattr(S, "Event", _Fake)
+    s._alloc_host(2 * s.max_reauth)
     s.flight, s.layout_dirty, s.next_chunk, s.steps, s.rows_active = [], False, 0, 0, 0
     s.stats = collections.Counter()
     appended = []
     s.append = lambda code, mask: appended.append(s.db_len) or setattr(s, "db_len", s.db_len + 1)
-    s.run_reauth = lambda items: [S.Completion(i, a, a, S.Result(reauth_match=False)) for i, a, _ in items]
+    s._launch_reauth = lambda items: (lambda now: [S.Completion(i, a, now, S.Result(reauth_match=False))
+                                                   for i, a, _ in items])
     return s, appended
 
 
