@@ -292,7 +292,7 @@ def run_ours(args):
         reqs = request_mix(nb, bc, bm, bpl, M, seed=7)
         lay = pack([list(centred_rotations(r.n_rot)) for r in reqs if r.kind == "uniqueness"
                     for _ in range(2 if r.mirrored else 1)])
-        q_cap = max(n_rows, (lay.n_rows + 63) // 64 * 64)
+        q_cap = max(n_rows, -(-lay.n_rows // 256) * 256)  # room for the 256-row tile padding
     ce = [irisb200.ShareDB(p, dm, M, q_cap, K_CODE, seeds[p]) for p in range(3)]
     me = [irisb200.ShareDB(p, dm, M, q_cap, K_MASK, seeds[p]) for p in range(3)]
     for e in ce + me:

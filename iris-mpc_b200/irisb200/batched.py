@@ -103,6 +103,18 @@ def pack(variant_rows: list) -> Layout:
                   np.array(seg_mask, np.uint32), n_slots * 32, n_slots)
 
 
+def pad_rows(layout: Layout, cap: int) -> Layout:
+    """Pads the row table with empty rows to a multiple of 256 (the GEMM's
+    widest tile) when the engines have room; the segment table is unchanged,
+    so the threshold kernel still visits only the packed slots."""
+    n = min(-(-layout.n_rows // 256) * 256, max(cap // 64 * 64, layout.n_rows))
+    if n <= layout.n_rows:
+        return layout
+    rd = np.full(n, 0xFFFFFFFF, np.uint32)
+    rd[: layout.n_rows] = layout.row_desc
+    return Layout(rd, layout.seg_start, layout.seg_query, layout.seg_mask, n, layout.n_slots)
+
+
 class BatchedEngine:
     """Runs batches of Requests against the six resident engines (party p code
     at code_engines[p], mask at mask_engines[p])."""
@@ -222,7 +234,8 @@ class BatchedEngine:
         return code, mask
 
     def _run_uniqueness(self, requests, variants, results):
-        layout = pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants])
+        layout = pad_rows(pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants]),
+                          self.ce[0].query_length)
         code, mask = self._base(requests, variants)
         for p in range(3):
             self.ce[p].query_upload_rows(code[p], layout.row_desc)

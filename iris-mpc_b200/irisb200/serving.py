@@ -248,7 +248,11 @@ class ContinuousServer:
         """Row table and segment table of the current placement."""
         used = [s for s in range(self.n_slot_cap) if self.slot_occ[s]]
         n_slots = used[-1] + 1 if used else 1
-        row_desc = np.full(n_slots * 32, 0xFFFFFFFF, np.uint32)
+        # the GEMM runs its widest tile (256 query rows) when the padded row count
+        # is a multiple of 256: pad with empty rows (the threshold kernel only
+        # visits the slots that carry segments)
+        n_rows = min(-(-n_slots * 32 // 256) * 256, self.row_capacity)
+        row_desc = np.full(n_rows, 0xFFFFFFFF, np.uint32)
         seg_start, seg_query, seg_mask = [0], [], []
         for s in range(n_slots):
             for v in sorted(self.slot_vars[s], key=lambda x: x.first):
