@@ -31,6 +31,7 @@ def test_first_run():
 def _placer(n_slots):
     s = ContinuousServer.__new__(ContinuousServer)
     s.n_slot_cap = n_slots
+    s.row_capacity = 32 * n_slots
     s.slot_occ = [0] * n_slots
     s.slot_vars = [[] for _ in range(n_slots)]
     return s
@@ -60,10 +61,12 @@ def test_placement_and_tables():
     for v in vs:
         used[v.slot * 32 + v.first: v.slot * 32 + v.first + len(v.rots)] = True
     assert (row_desc[~used] == 0xFFFFFFFF).all()
-    # releasing frees exactly the rows; the table shrinks to the last used word
+    # releasing frees exactly the rows; the segment table shrinks to the last used
+    # word while the row table stays padded towards the 256-row GEMM tile
     s._release(vs[6])
     assert s.slot_occ[3] == 0
-    assert s._layout()[0].size == 96
+    rd, st, _, _ = s._layout()
+    assert st.size - 1 == 3 and rd.size == 128 and (rd[96:] == 0xFFFFFFFF).all()
     assert s._place(31) == (3, 0)
 
 
