@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: arrival window per load")
     ap.add_argument("--chunk", type=int, default=65536, help="serving: DB chunk per step")
     ap.add_argument("--serving-arms", default="served,plain", help="serving: which servers to run")
+    ap.add_argument("--serving-rate", type=float, default=500.0,
+                    help="default run: offered load of its serving leg, requests/s (0 = skip)")
     return ap.parse_args()
 
 
@@ -296,7 +298,7 @@ def run_ours(args):
     ce = [irisb200.ShareDB(p, dm, M, q_cap, K_CODE, seeds[p]) for p in range(3)]
     me = [irisb200.ShareDB(p, dm, M, q_cap, K_MASK, seeds[p]) for p in range(3)]
     for e in ce + me:
-        e.alloc_db(M)
+        e.alloc_db(M + 256)  # room for the serving leg's appends
     t0 = time.perf_counter()
     irisb200.synth_db(ce, me, DB_SEED + rank, 0, M)
     synth_s = time.perf_counter() - t0
@@ -444,6 +446,27 @@ def run_ours(args):
             "planted_matches_found": f"{planted_hits}/{planted_uniq}",
             "clocks": clk.summary(clk.windows[-1]),
         }
+
+    # ---------------- serving leg: continuous batching under Poisson arrivals ----------------
+    serving = None
+    if reqs and args.serving_rate > 0:
+        from irisb200.serving import ContinuousServer
+        nq_s = 512
+        spl = {j: (int((j * 7919 + 13) % M), (j * 7) % 31 - 15) for j in range(0, nq_s, 10)}
+        sqc, sqm = irisb200.synth_queries(DB_SEED + rank, Q_SEED + 2, nq_s, spl)
+        app_c, app_m = append_records(ce, me, M)
+        srv = ContinuousServer(dm, ce, me, c, chunk=65536, row_capacity=q_cap, max_variants=min(q_cap // 2, 2048),
+                               max_reauth=64, threshold_a=A, seeds=seeds, db_capacity=M + 256)
+        warm = request_mix(40, sqc, sqm, spl, M, seed=99)
+        srv.serve([0.0] * len(warm), warm)
+        serving = serve_load(srv, srv, args.serving_rate, 2.0, 0, (sqc, sqm, spl, M, app_c, app_m), clk)
+        serving["vs_plain_value"] = serving["comparisons_per_s"] / value
+        serving["config"] = {"workload": "continuous serving: Poisson arrivals, 80% uniqueness / 20% reauth, 1% "
+                                         "appends, rotations 1/16/31, 50% mirrored, 2 s of arrivals",
+                             "row_capacity": q_cap, "chunk": 65536}
+        srv.close()
+        for e in ce + me:
+            e.set_db_len(M)
     clk.__exit__(None, None, None)
 
     result = None
@@ -494,6 +517,8 @@ def run_ours(args):
         }
         if batched:
             result["batched"] = batched
+        if serving:
+            result["serving"] = serving
         mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
         rf = result["roofline"]
         if os.path.exists(mp):
@@ -533,6 +558,51 @@ def _latency_stats(comps, requests, t0, db_lens):
             "requests_per_s": len(comps) / (end - t0), "comparisons_per_s": work / (end - t0)}
 
 
+def append_records(ce, me, M, n=64, seed=3):
+    """Records for append requests: copies of existing irises (re-enrolments),
+    [3][n][K] code and mask shares, fetched before any timing."""
+    import numpy as np
+    ids = [int(x) for x in np.random.default_rng(seed).integers(0, M, n)]
+    c = np.stack([np.stack([ce[p].fetch_records(e, 1)[0] for e in ids]) for p in range(3)])
+    m = np.stack([np.stack([me[p].fetch_records(e, 1)[0] for e in ids]) for p in range(3)])
+    return c, m
+
+
+def serve_load(server, stats_src, lam, seconds, seed, pool, clk):
+    """One open-loop Poisson run at `lam` requests/s for `seconds` of arrivals
+    (80% uniqueness / 20% reauth, 1% appends, rotations 1/16/31, 50% mirrored)
+    through server.serve; returns the latency and throughput figures."""
+    import numpy as np
+    qc, qm, planted, M, app_c, app_m = pool
+    rng = np.random.default_rng(1000 + seed)
+    n = max(20, int(lam * seconds))
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, n)).tolist()
+    reqs = request_mix(n, qc, qm, planted, M, seed=2000 + seed, p_append=0.01)
+    appends = {i: (app_c[:, i % app_c.shape[1]], app_m[:, i % app_c.shape[1]])
+               for i, r in enumerate(reqs) if r.kind == "append"}
+    lens, cur = [], server.db_len  # each request's DB scope: the appends that arrived before it
+    for r in reqs:
+        if r.kind == "append":
+            cur += 1
+        lens.append(cur)
+    stats0 = dict(stats_src.stats) if stats_src else {}
+    with clk.mark():
+        t0 = time.perf_counter()
+        comps = server.serve(arrivals, reqs, appends=appends, max_wall_s=300.0)
+    st = _latency_stats(comps, reqs, t0, lens)
+    st.update(offered_requests_per_s=lam, requests=n, appends=len(appends),
+              reauth=sum(r.kind == "reauth" for r in reqs), clocks=clk.summary(clk.windows[-1]))
+    if stats_src:
+        d = {k: stats_src.stats[k] - stats0.get(k, 0) for k in stats_src.stats}
+        n_st = max(1, d.get("steps", 0))
+        st["steps"] = d.get("steps", 0)
+        st["mean_rows_per_step"] = d.get("rows", 0) / n_st
+        st["mean_used_rows_per_step"] = d.get("used_rows", 0) / n_st
+        st["mean_step_interval_ms"] = (max(c.done for c in comps) - t0) * 1e3 / n_st
+        st["host_s"] = {k: round(d.get(k, 0.0), 3) for k in ("launch_s", "layout_s", "wait_s")}
+    return st
+
+
 def run_serving(args):
     """Poisson arrivals against the resident 512K-entry DB: the continuous
     server and the plain batch-at-a-time drop-in at each offered load."""
@@ -566,10 +636,7 @@ def run_serving(args):
     nq = 512
     planted = {j: (int((j * 7919 + 13) % M), (j * 7) % 31 - 15) for j in range(0, nq, 10)}
     qc, qm = irisb200.synth_queries(DB_SEED, Q_SEED + 2, nq, planted)
-    # append records: copies of existing irises (re-enrolments), fetched before any timing
-    app_ids = [int(x) for x in np.random.default_rng(3).integers(0, M, 64)]
-    app_c = np.stack([np.stack([ce[p].fetch_records(e, 1)[0] for e in app_ids]) for p in range(3)])  # [3][64][K]
-    app_m = np.stack([np.stack([me[p].fetch_records(e, 1)[0] for e in app_ids]) for p in range(3)])
+    app_c, app_m = append_records(ce, me, M)
     max_var = min(R // 2, 4096)
     srv = ContinuousServer(dm, ce, me, c, chunk=chunk, row_capacity=R, max_variants=max_var, max_reauth=64,
                            threshold_a=A, seeds=seeds, db_capacity=cap)
@@ -580,39 +647,14 @@ def run_serving(args):
     plain.serve([0.0] * len(warm), warm)
     clk = ClockSampler(0).__enter__()
     time.sleep(2.0)
+    pool = (qc, qm, planted, M, app_c, app_m)
     sweep = []
     for li, lam in enumerate(rates):
-        rng = np.random.default_rng(1000 + li)
-        n = max(20, int(lam * args.serve_seconds))
-        arrivals = np.cumsum(rng.exponential(1.0 / lam, n)).tolist()
-        reqs = request_mix(n, qc, qm, planted, M, seed=2000 + li, p_append=0.01)
-        appends = {i: (app_c[:, i % 64], app_m[:, i % 64]) for i, r in enumerate(reqs) if r.kind == "append"}
-        row = {"offered_requests_per_s": lam, "requests": n,
-               "appends": len(appends), "reauth": sum(r.kind == "reauth" for r in reqs)}
+        row = {"offered_requests_per_s": lam}
         arms = [a for a in (("served", srv), ("plain", plain)) if a[0] in args.serving_arms.split(",")]
         for name, server in arms:
-            db0 = server.db_len
-            # each request's DB scope: the DB length after the appends that arrived before it
-            lens, cur = [], db0
-            for r in reqs:
-                if r.kind == "append":
-                    cur += 1
-                lens.append(cur)
-            stats0 = dict(srv.stats)
-            with clk.mark():
-                t0 = time.perf_counter()
-                comps = server.serve(arrivals, reqs, appends=appends, max_wall_s=300.0)
-            st = _latency_stats(comps, reqs, t0, lens)
-            st["clocks"] = clk.summary(clk.windows[-1])
-            if name == "served":
-                d = {k: srv.stats[k] - stats0.get(k, 0) for k in srv.stats}
-                n_st = max(1, d.get("steps", 0))
-                st["steps"] = d.get("steps", 0)
-                st["mean_rows_per_step"] = d.get("rows", 0) / n_st
-                st["mean_used_rows_per_step"] = d.get("used_rows", 0) / n_st
-                st["mean_step_interval_ms"] = (max(c.done for c in comps) - t0) * 1e3 / n_st
-                st["host_s"] = {k: round(d.get(k, 0.0), 3) for k in ("launch_s", "layout_s", "wait_s")}
-            row[name] = st
+            row[name] = serve_load(server, srv if name == "served" else None, lam, args.serve_seconds, li, pool,
+                                   clk)
         if "served" in row and "plain" in row:
             row["served_vs_plain_comparisons"] = (row["served"]["comparisons_per_s"] /
                                                   row["plain"]["comparisons_per_s"])
