@@ -59,8 +59,9 @@ def parse():
     ap.add_argument("--threshold-a", type=int, default=16384)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cublas", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "serving"],
-                    help="plain: the drop-in batch (+ the batched uneven leg); serving: Poisson sweep")
+    ap.add_argument("--mode", default="plain", choices=["plain", "serving", "sweep"],
+                    help="plain: the drop-in batch (+ batched and serving legs); serving: Poisson sweep; "
+                         "sweep: single-party GEMM and comparison-kernel roofline sweep")
     ap.add_argument("--batched-requests", type=int, default=256, help="requests per batched-leg batch (0 = skip)")
     ap.add_argument("--rates", default="50,200,500,1000,2000", help="serving: offered loads, requests/s")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: arrival window per load")
@@ -704,12 +705,96 @@ def run_serving(args):
     dm.close()
 
 
+def run_sweep(args):
+    """Single-party limb GEMM over query rows x DB entries (K = 12800, as the
+    reference's matmul bench) and the 3-party comparison kernel over element
+    counts, each against its roofline."""
+    import numpy as np
+    import torch
+
+    import irisb200
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    dm = irisb200.DeviceManager(0)
+    s0 = torch.cuda.ExternalStream(dm.stream(0), device=torch.device("cuda", 0))
+    mp = {}
+    if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")):
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mp = json.load(f)
+    hbm = mp.get("hbm_gbs", 6650.0) * 1e9
+    int8_peak = 2 * mp.get("bf16_tflops", 1590.0) * 1e12
+
+    def timed(fn, reps):
+        fn()
+        dm.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s0)
+        for _ in range(reps):
+            fn()
+        b.record(s0)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    clk = ClockSampler(0).__enter__()
+    time.sleep(2.0)
+    gemm = []
+    qs, ms = (64, 256, 1024), (262144, 1048576, 2097152)
+    seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
+    eng = irisb200.ShareDB(0, dm, max(ms), max(qs), K_CODE, seeds[0])
+    eng.alloc_db(max(ms))
+    eng.fill_random(DB_SEED, max(ms))
+    rng = np.random.default_rng(5)
+    for q in qs:
+        eng.query_upload(rng.integers(0, 65536, (q, K_CODE), dtype=np.uint16))
+        for m in ms:
+            with clk.mark():
+                t = timed(lambda: eng.dot(0, m, 1, dm.stream(0)), 3)
+            ops = 6 * K_CODE * q * m
+            bound = min(int8_peak, 3 * q * hbm)
+            gemm.append({"query_rows": q, "db_entries": m, "ms": t, "tops": ops / t / 1e9,
+                         "bound": "hbm" if 3 * q * hbm < int8_peak else "tensor",
+                         "frac": ops / (t * 1e-3) / bound, "clocks": clk.summary(clk.windows[-1])})
+    eng.close()
+    cmp_ = []
+    c = irisb200.Circuits(dm, seeds)
+    for e in (1 << 20, 1 << 23, 1 << 27, 1 << 30):
+        bufs = [irisb200.DeviceBuffer(dm, 2 * e) for _ in range(6)]
+        for i, b in enumerate(bufs):
+            b.fill_random(1000 + i)
+        ra = [irisb200.DeviceBuffer(dm, e // 8) for _ in range(3)]
+        rb = [irisb200.DeviceBuffer(dm, e // 8) for _ in range(3)]
+        op = irisb200.DeviceBuffer(dm, e // 8)
+        with clk.mark():
+            t = timed(lambda: c.compare_threshold_masked_many(bufs[:3], bufs[3:], e, 16384, ra, rb, op,
+                                                              dm.stream(0)), 3)
+        algo = e * 12 + e * 7 // 8  # 3 parties x (code + mask) u16 read; (a, b) bits x 3 + opened bits written
+        cmp_.append({"elements": e, "ms": t, "elements_per_s": e / (t * 1e-3), "gbs": algo / t / 1e6,
+                     "frac_hbm": algo / (t * 1e-3) / hbm, "bound": "alu (ChaCha12 + bit-sliced circuits)",
+                     "clocks": clk.summary(clk.windows[-1])})
+        for b in bufs + ra + rb + [op]:
+            b.free()
+    c.close()
+    clk.__exit__(None, None, None)
+    print(json.dumps({"metric": "limb GEMM TOPS and comparison elements/s (roofline sweep)", "value": None,
+                      "unit": "TOPS", "n_gpus": 1, "data": "synthetic",
+                      "config": {"workload": "single-party limb GEMM, K = 12800, query rows x DB entries; "
+                                             "3-party compare_threshold_masked_many over element counts",
+                                 "int8_peak_tops": int8_peak / 1e12, "hbm_gbs": hbm / 1e9,
+                                 "peak_source": "MEASURED_PEAKS.json: 2 x bf16 burst, hbm_gbs"},
+                      "gemm": gemm, "comparison": cmp_}), flush=True)
+    dm.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.mode == "serving":
         run_serving(args)
+    elif args.mode == "sweep":
+        run_sweep(args)
     else:
         run_ours(args)
 

@@ -142,6 +142,12 @@ int irs_sharedb_db_len(irs_sharedb* db, size_t* len);
 int irs_sharedb_synth_db(irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3], uint64_t seed,
                          size_t first, size_t n);
 
+/* Records 0..n-1 of one engine filled with seeded uniform limb bytes (a
+ * single-engine benchmark DB: the GEMM sweep of matmul.rs has no encoding). */
+int irs_sharedb_fill_random(irs_sharedb* db, uint64_t seed, size_t n);
+/* Seeded uniform bytes in a device buffer (8-byte aligned, bytes % 8 == 0). */
+int irs_device_fill_random(void* ptr, size_t bytes, uint64_t seed, void* stream);
+
 /* preprocess_iris_code_query_share / preprocess_mask_code_query_share
  * (galois_engine.rs:23-40,193-195,438-440) on the host, in place: each GR4
  * block times the party's Lagrange coefficient at 0, converted to basis B. */

@@ -614,6 +614,28 @@ static cudaError_t wait_last_dot(irs_sharedb* db, cudaStream_t s) {
   return cudaStreamWaitEvent(s, db->dm->graph_done, 0);
 }
 
+int irs_sharedb_fill_random(irs_sharedb* db, uint64_t seed, size_t n) {
+  CHECK(db && db->db_lo, IRS_ERR_STATE, "alloc_db not called");
+  CHECK(n <= db->db_cap, IRS_ERR_INVALID, "%zu records exceed the DB capacity %zu", n, db->db_cap);
+  CHECK((n * db->code_length) % 8 == 0, IRS_ERR_INVALID, "records x code_length must be a multiple of 8");
+  irs_device_manager* dm = db->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[db->peer];
+  CU(wait_last_dot(db, s));
+  CU(launch_fill_random(db->db_lo, n * db->code_length, seed, s));
+  CU(launch_fill_random(db->db_hi, n * db->code_length, seed ^ 0x5A5A5A5A5A5A5A5Aull, s));
+  CU(cudaStreamSynchronize(s));
+  db->db_len = std::max(db->db_len, n);
+  return IRS_OK;
+}
+
+int irs_device_fill_random(void* ptr, size_t bytes, uint64_t seed, void* stream) {
+  CHECK(ptr && bytes % 8 == 0 && reinterpret_cast<uintptr_t>(ptr) % 8 == 0, IRS_ERR_INVALID,
+        "8-byte aligned pointer and a multiple of 8 bytes needed");
+  CU(launch_fill_random(ptr, bytes, seed, static_cast<cudaStream_t>(stream)));
+  return IRS_OK;
+}
+
 int irs_sharedb_query_upload(irs_sharedb* db, const uint16_t* rows, size_t n_rows) {
   CHECK(db && (rows || !n_rows), IRS_ERR_INVALID, "bad arguments");
   int rc = set_active_rows(db, n_rows);

@@ -132,6 +132,17 @@ __device__ __forceinline__ void gr4_mul(const uint32_t a[4], const uint32_t b[4]
 // One CTA per entry.  Mirrors the synthetic generator and the degree-1 Shamir
 // encoding the CPU oracle defines (iris bits from rng64, mask pairs kept with
 // probability 0.9, share randomness r = rng64(share seed, block)).
+// Seeded uniform bytes (splitmix64 of the 8-byte word index): random shares
+// for benchmark buffers whose values do not matter, only their bit activity.
+__global__ void fill_random_kernel(uint64_t* __restrict__ p, size_t n_words, uint64_t seed) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_words; i += (size_t)gridDim.x * blockDim.x) {
+    uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    p[i] = z ^ (z >> 31);
+  }
+}
+
 __global__ void synth_db_kernel(uint64_t seed, uint32_t first, uint32_t count, SynthOut out) {
   __shared__ uint64_t code[200], mask[200];
   const uint32_t e = first + blockIdx.x;
@@ -228,6 +239,15 @@ cudaError_t launch_gather_rows(const uint8_t* src_lo, const uint8_t* src_hi, con
   const size_t total = (size_t)n * (K / 16);
   if (!total) return cudaSuccess;
   gather_rows_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(src_lo, src_hi, ids, n, K, dst_lo, dst_hi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_random(void* p, size_t bytes, uint64_t seed, cudaStream_t stream) {
+  const size_t n = bytes / 8;
+  if (n) {
+    const size_t blocks = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
+    fill_random_kernel<<<(unsigned)blocks, 256, 0, stream>>>(static_cast<uint64_t*>(p), n, seed);
+  }
   return cudaGetLastError();
 }
 

@@ -29,6 +29,7 @@ cudaError_t launch_expand_rows(const uint16_t* base, uint32_t K, const uint32_t*
                                uint32_t n_pad, uint8_t* lo, uint8_t* hi, cudaStream_t stream);
 cudaError_t launch_gather_rows(const uint8_t* src_lo, const uint8_t* src_hi, const uint32_t* ids, uint32_t n,
                                uint32_t K, uint8_t* dst_lo, uint8_t* dst_hi, cudaStream_t stream);
+cudaError_t launch_fill_random(void* p, size_t bytes, uint64_t seed, cudaStream_t stream);
 cudaError_t launch_synth_db(uint64_t seed, uint32_t first, uint32_t count, const SynthOut& out, cudaStream_t stream);
 
 }  // namespace irs

@@ -95,6 +95,8 @@ _SIGS = {
     "irs_device_manager_advance_batch_counter": [_vp, _vp],
     "irs_sharedb_query_upload_rows": [_vp, _vp, _sz, _vp, _sz],
     "irs_sharedb_gather_records": [_vp, _vp, _vp, _sz],
+    "irs_sharedb_fill_random": [_vp, _u64, _sz],
+    "irs_device_fill_random": [_vp, _sz, _u64, _vp],
     "irs_sharedb_query_put_base": [_vp, _sz, _sz, _vp],
     "irs_sharedb_query_expand_rows": [_vp, _sz, _vp, _sz],
     "irs_mirror_query_share": [_vp, _sz, _i],
@@ -192,6 +194,9 @@ class DeviceBuffer:
         _check(lib().irs_copy_d2h(_ptr(out), self.ptr, out.nbytes, stream))
         _check(lib().irs_stream_synchronize(stream))
         return out
+
+    def fill_random(self, seed: int, stream=None) -> None:
+        _check(lib().irs_device_fill_random(self.ptr, self.nbytes // 8 * 8, seed, stream))
 
     def free(self) -> None:
         if self.ptr:
@@ -435,6 +440,10 @@ class ShareDB:
         """query_upload_rows over the resident pool [0, n_base)."""
         rd = np.ascontiguousarray(row_desc, np.uint32)
         _check(lib().irs_sharedb_query_expand_rows(self.h, n_base, _ptr(rd), rd.size))
+
+    def fill_random(self, seed: int, n: int) -> None:
+        """Records 0..n-1 filled with seeded uniform limb bytes (benchmark DB)."""
+        _check(lib().irs_sharedb_fill_random(self.h, seed, n))
 
     def gather_records(self, src: "ShareDB", ids) -> None:
         """prefetch_subset: records ids[k] of src become records k of this engine."""
