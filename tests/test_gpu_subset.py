@@ -1,0 +1,75 @@
+"""Two-stage check: a full scan at the prefilter ratio 0.375 collects the
+batch's candidates, the subset pass re-checks the batch against only those
+entries at 0.345 (compare_query_against_db_subset_and_self,
+iris-mpc-gpu/src/server/actor.rs:1900-2244).  Because every 0.345 match is a
+0.375 match, the two-stage result must equal a full scan at 0.345, entry for
+entry, and the subset pass on the other eye must equal that eye's full scan
+restricted to the same candidates.  Subsets larger than one chunk are split."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import irisb200
+from irisb200.subset import SubsetPass
+import workload as W
+
+pytestmark = pytest.mark.gpu
+
+N_DB, NQ = 1500, 8
+
+
+def _engines(dm, oracle, db_seed, q_seed, planted):
+    codes, masks, cs, ms = W.make_db(oracle, N_DB, db_seed)
+    qc, qm, _ = W.make_queries(oracle, NQ, codes, masks, q_seed, planted)
+    ce = [irisb200.ShareDB(p, dm, N_DB, NQ * 32, 12800, W.SEEDS[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, N_DB, NQ * 32, 6400, W.SEEDS[p]) for p in range(3)]
+    for p in range(3):
+        ce[p].alloc_db(N_DB)
+        me[p].alloc_db(N_DB)
+        ce[p].load_records(0, cs[p])
+        me[p].load_records(0, ms[p])
+    return ce, me, cs, ms, qc, qm
+
+
+def test_two_stage_equals_full_scan(dm, oracle):
+    # planted near-duplicates; 0.2-flip copies match at both ratios, and query 5
+    # duplicates entries 40 and 1400 so that several candidates share a query
+    left = _engines(dm, oracle, 0xA11CE, 31, {0: (7, 0), 1: (640, 4), 3: (1499, -6), 5: (40, 0), 6: (1400, 1)})
+    right = _engines(dm, oracle, 0xB0B, 32, {0: (7, 1), 1: (900, 0), 3: (1499, 0), 6: (1400, -2)})
+    c = irisb200.Circuits(dm, W.SEEDS)
+    sp_l = SubsetPass(dm, left[0], left[1], c, max_queries=NQ, max_subset=3)  # tiny chunks: exercises splitting
+    sp_r = SubsetPass(dm, right[0], right[1], c, max_queries=NQ, max_subset=64)
+    try:
+        ce, me, cs, ms, qc, qm = left
+        # stage 1: full scan of the left eye at the prefilter ratio
+        pre = W.expected_bitmap(oracle, qc, qm, cs, ms, irisb200.THRESHOLD_ANON_STATS_A)
+        dc = irisb200.DistanceComparator(dm, NQ, N_DB)
+        slots = [(j, 0, 31, j) for j in range(NQ)]
+        for p in range(3):
+            ce[p].query_upload_slots(qc[p], slots)
+            me[p].query_upload_slots(qm[p], slots)
+        irisb200.dot_many(ce + me, [1, 1, 1, 2, 2, 2], 0, N_DB)
+        dc.compare_threshold_open(c, ce, me, 0, N_DB, NQ, irisb200.THRESHOLD_ANON_STATS_A)
+        counts, pos = dc.take_rows(np.arange(NQ, dtype=np.uint32), N_DB)
+        cand = sorted({int(e) for q in range(NQ) for e in pos[q, : int(counts[q])]})
+        assert cand == sorted(set(np.nonzero(pre.any(axis=0))[0].tolist()))
+        dc.close()
+        # stage 2: the subset pass at the match ratio, both eyes, same candidates
+        got_l = sp_l.run(qc, qm, cand, irisb200.THRESHOLD_A)
+        full_l = W.expected_bitmap(oracle, qc, qm, cs, ms, irisb200.THRESHOLD_A)
+        for q in range(NQ):
+            assert got_l[q] == np.nonzero(full_l[q])[0].tolist(), f"left query {q}"
+        _, _, csr, msr, qcr, qmr = right
+        got_r = sp_r.run(qcr, qmr, cand, irisb200.THRESHOLD_A)
+        full_r = W.expected_bitmap(oracle, qcr, qmr, csr, msr, irisb200.THRESHOLD_A)
+        for q in range(NQ):
+            assert got_r[q] == [e for e in np.nonzero(full_r[q])[0].tolist() if e in cand], f"right query {q}"
+        assert 7 in got_l[0] and 7 in got_r[0] and 1499 in got_l[3] and 1499 in got_r[3]
+        assert got_l[2] == [] and sp_l.run(qc, qm, [], irisb200.THRESHOLD_A) == [[] for _ in range(NQ)]
+    finally:
+        sp_l.close()
+        sp_r.close()
+        c.close()
+        for e in left[0] + left[1] + right[0] + right[1]:
+            e.close()
