@@ -59,9 +59,11 @@ def parse():
     ap.add_argument("--threshold-a", type=int, default=16384)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cublas", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "serving", "sweep"],
+    ap.add_argument("--mode", default="plain", choices=["plain", "serving", "sweep", "batched"],
                     help="plain: the drop-in batch (+ batched and serving legs); serving: Poisson sweep; "
-                         "sweep: single-party GEMM and comparison-kernel roofline sweep")
+                         "sweep: single-party GEMM and comparison-kernel roofline sweep; "
+                         "batched: batch sizes --batch-sizes, batched engine vs plain slots")
+    ap.add_argument("--batch-sizes", default="1,16,64,256", help="batched mode: requests per batch")
     ap.add_argument("--batched-requests", type=int, default=256, help="requests per batched-leg batch (0 = skip)")
     ap.add_argument("--rates", default="50,200,500,1000,2000", help="serving: offered loads, requests/s")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: arrival window per load")
@@ -787,6 +789,115 @@ def run_sweep(args):
     dm.close()
 
 
+def run_batched_sweep(args):
+    """Config 3 over batch sizes: the same seeded request batches through the
+    batched engine (packed rows, graphs, autotuner) and through the plain
+    drop-in (every orientation in a 31-rotation slot, 64 slots per batch,
+    reauth requests scanned against the whole DB as the plain path does)."""
+    import numpy as np
+    import torch
+
+    import irisb200
+    from irisb200.batched import BatchedEngine, centred_rotations, pack, pad_rows
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    M, A = args.db, args.threshold_a
+    sizes = [int(x) for x in args.batch_sizes.split(",") if x]
+    seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
+    nb = max(sizes)
+    pl = {j: (int((j * 104729 + 7) % M), (j * 5) % 31 - 15) for j in range(0, nb, 10)}
+    qc, qm = irisb200.synth_queries(DB_SEED, Q_SEED + 1, nb, pl)
+    mixes = {b: request_mix(b, qc, qm, pl, M, seed=7 + b) for b in sizes}
+    rows = max(-(-pad_rows(pack([list(centred_rotations(r.n_rot)) for r in mixes[b] if r.kind == "uniqueness"
+                                  for _ in range(2 if r.mirrored else 1)]), 1 << 20).n_rows // 256) * 256
+               for b in sizes)
+    q_cap = max(2048, rows)
+    dm = irisb200.DeviceManager(0)
+    ce = [irisb200.ShareDB(p, dm, M, q_cap, K_CODE, seeds[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, M, q_cap, K_MASK, seeds[p]) for p in range(3)]
+    for e in ce + me:
+        e.alloc_db(M)
+    irisb200.synth_db(ce, me, DB_SEED, 0, M)
+    c = irisb200.Circuits(dm, seeds)
+    dc = irisb200.DistanceComparator(dm, 64, M)
+    clk = ClockSampler(0).__enter__()
+    time.sleep(2.0)
+    out = []
+    for b in sizes:
+        reqs = mixes[b]
+        n_var = sum(2 if r.mirrored else 1 for r in reqs if r.kind == "uniqueness")
+        n_re = sum(2 if r.mirrored else 1 for r in reqs if r.kind == "reauth")
+        eng = BatchedEngine(dm, ce, me, c, max_variants=max(64, n_var), max_reauth=max(16, n_re), threshold_a=A,
+                            seeds=seeds)
+        for _ in range(2):
+            eng.run(reqs)
+        lat = []
+        with clk.mark():
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                eng.run(reqs)
+                lat.append((time.perf_counter() - t0) * 1e3)
+        bclk = clk.summary(clk.windows[-1])
+        eng.close()
+        comps = sum(comparisons_of(r, M) for r in reqs)
+        # the plain drop-in on the same requests: every orientation in a 31-rotation slot
+        base_c, base_m = [], []
+        for r in reqs:
+            for mir in ([False, True] if r.mirrored else [False]):
+                base_c.append([irisb200.mirror_query_share(r.code[p], True) if mir else r.code[p] for p in range(3)])
+                base_m.append([irisb200.mirror_query_share(r.mask[p], False) if mir else r.mask[p] for p in range(3)])
+        bc = np.ascontiguousarray(np.array(base_c, np.uint16).transpose(1, 0, 2))
+        bm = np.ascontiguousarray(np.array(base_m, np.uint16).transpose(1, 0, 2))
+        for e in ce + me:
+            e.use_batch_counter(False)
+            e.set_tile(0)
+        c.use_batch_counter(False)
+
+        def plain_pass():
+            for s0 in range(0, bc.shape[1], 64):
+                n = min(64, bc.shape[1] - s0)
+                slots = [(j, 0, 31, j) for j in range(n)]
+                for p in range(3):
+                    ce[p].query_upload_slots(bc[p, s0:s0 + n], slots)
+                    me[p].query_upload_slots(bm[p, s0:s0 + n], slots)
+                dc.reset()
+                irisb200.dot_many(ce + me, [1, 1, 1, 2, 2, 2], 0, M)
+                dc.compare_threshold_open(c, ce, me, 0, M, n, A)
+                dc.join_db_matches(n, M)
+                dc.fetch_final_results(n)
+        plain_pass()
+        plat = []
+        with clk.mark():
+            for _ in range(max(1, args.steps // 2)):
+                t0 = time.perf_counter()
+                plain_pass()
+                plat.append((time.perf_counter() - t0) * 1e3)
+        pclk = clk.summary(clk.windows[-1])
+        lat.sort()
+        plat.sort()
+        out.append({"requests": b, "uniqueness_orientations": n_var, "reauth_orientations": n_re,
+                    "comparisons_per_batch": comps,
+                    "batched": {"comparisons_per_s": comps / (statistics.mean(lat) * 1e-3), "p50_ms": lat[len(lat) // 2],
+                                "p99_ms": lat[-1], "clocks": bclk},
+                    "plain": {"comparisons_per_s": comps / (statistics.mean(plat) * 1e-3),
+                              "p50_ms": plat[len(plat) // 2], "p99_ms": plat[-1], "slot_batches": -(-bc.shape[1] // 64),
+                              "clocks": pclk}})
+        out[-1]["batched_vs_plain"] = out[-1]["batched"]["comparisons_per_s"] / out[-1]["plain"]["comparisons_per_s"]
+    clk.__exit__(None, None, None)
+    print(json.dumps({"metric": "iris comparisons/sec (3-party, 1 B200) batched vs plain; p50/p99 batch latency",
+                      "value": None, "unit": UNIT, "n_gpus": 1, "data": "synthetic",
+                      "config": {"workload": f"batched uneven launches over batch sizes, {M} entries per party, "
+                                             "rotations 1/16/31, 50% mirrored, 80% uniqueness / 20% reauth",
+                                 "timing": "host wall clock per batch, queries uploaded from host memory, "
+                                           "match lists returned"},
+                      "sizes": out}), flush=True)
+    for o in ce + me + [c, dc]:
+        o.close()
+    dm.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -795,6 +906,8 @@ def main():
         run_serving(args)
     elif args.mode == "sweep":
         run_sweep(args)
+    elif args.mode == "batched":
+        run_batched_sweep(args)
     else:
         run_ours(args)
 
