@@ -103,11 +103,19 @@ def pack(variant_rows: list) -> Layout:
                   np.array(seg_mask, np.uint32), n_slots * 32, n_slots)
 
 
+def padded_rows(n_rows: int, cap: int) -> int:
+    """Query rows to run for `n_rows` packed rows: above 256 rows the GEMM is
+    tensor-bound and pads to a multiple of 256 (its widest tile); below, it is
+    bound by streaming the DB and keeps the fewest rows (multiple of 64)."""
+    if n_rows <= 256:
+        return -(-n_rows // 64) * 64
+    return min(-(-n_rows // 256) * 256, max(cap // 64 * 64, n_rows))
+
+
 def pad_rows(layout: Layout, cap: int) -> Layout:
-    """Pads the row table with empty rows to a multiple of 256 (the GEMM's
-    widest tile) when the engines have room; the segment table is unchanged,
-    so the threshold kernel still visits only the packed slots."""
-    n = min(-(-layout.n_rows // 256) * 256, max(cap // 64 * 64, layout.n_rows))
+    """Pads the row table with empty rows (padded_rows); the segment table is
+    unchanged, so the threshold kernel still visits only the packed slots."""
+    n = padded_rows(layout.n_rows, cap)
     if n <= layout.n_rows:
         return layout
     rd = np.full(n, 0xFFFFFFFF, np.uint32)

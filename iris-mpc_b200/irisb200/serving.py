@@ -37,7 +37,7 @@ import numpy as np
 
 from . import (IRIS_CODE_LENGTH, MASK_CODE_LENGTH, MAX_MATCHES_LEN, DistanceComparator, Event, IrisError,
                PinnedArray, ShareDB, dot_many, mirror_query_share)
-from .batched import MULTS, Request, Result, centred_rotations, pack
+from .batched import MULTS, Request, Result, centred_rotations, pack, padded_rows
 
 RESULT_BYTES_PER_ROW_ENTRY = 2 * 6  # u16 dot share per (row, entry) for 6 engines
 
@@ -248,10 +248,9 @@ class ContinuousServer:
         """Row table and segment table of the current placement."""
         used = [s for s in range(self.n_slot_cap) if self.slot_occ[s]]
         n_slots = used[-1] + 1 if used else 1
-        # the GEMM runs its widest tile (256 query rows) when the padded row count
-        # is a multiple of 256: pad with empty rows (the threshold kernel only
-        # visits the slots that carry segments)
-        n_rows = min(-(-n_slots * 32 // 256) * 256, self.row_capacity)
+        # empty rows pad the table for the GEMM's widest tile (padded_rows); the
+        # threshold kernel only visits the slots that carry segments
+        n_rows = min(padded_rows(n_slots * 32, self.row_capacity), self.row_capacity)
         row_desc = np.full(n_rows, 0xFFFFFFFF, np.uint32)
         seg_start, seg_query, seg_mask = [0], [], []
         for s in range(n_slots):
