@@ -327,6 +327,20 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
  * rows of completed requests).  Synchronous. */
 int irs_dc_take_rows(irs_distance_comparator* dc, const uint32_t* rows, size_t n, size_t db_len, int clear,
                      uint32_t* counts, uint32_t* ids);
+/* Anonymised-statistics distance capture (openResults' match distance
+ * buffers, iris-mpc-gpu/src/dot/kernel.cu:73-106; DistanceCache,
+ * server/anon_stats.rs): once enabled, every later compare_threshold_open(_prepared)
+ * of this comparator appends, for each opened match of a valid query row, the
+ * DB entry, the query row (32 * slot + row of the slot) and the three parties'
+ * additive components of the code and (x2) mask dot shares, up to `cap`
+ * records (further matches are counted, not stored).  Run it on the prefilter
+ * pass (IRS_THRESHOLD_ANON_STATS_A) as the reference does. */
+int irs_dc_enable_distance_capture(irs_distance_comparator* dc, size_t cap);
+/* Copies up to `cap` captured records: entry [cap], row [cap], code [3][cap],
+ * mask [3][cap] (component p at p * cap); *n = records captured so far
+ * (possibly above the capture capacity).  reset != 0 empties the capture. */
+int irs_dc_fetch_distances(irs_distance_comparator* dc, size_t cap, uint32_t* entry, uint32_t* row, uint16_t* code,
+                           uint16_t* mask, size_t* n, int reset);
 /* Clears bitmap rows [first, first + n) (a query row reused by the serving
  * loop for a new request). */
 int irs_dc_clear_rows(irs_distance_comparator* dc, size_t first, size_t n, void* stream);

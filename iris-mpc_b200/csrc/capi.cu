@@ -122,6 +122,9 @@ struct irs_distance_comparator {
   uint32_t* d_slot_valid = nullptr;
   uint32_t* d_slot_query = nullptr;
   uint32_t* d_take = nullptr;  // irs_dc_take_rows: row list [max_queries], counts [max_queries], ids [max_queries][256]
+  // distance capture (irs_dc_enable_distance_capture): count, entry, row, code [3], mask [3]
+  uint32_t* d_dist = nullptr;
+  size_t dist_cap = 0;
   size_t slot_cap = 0;
   // segment table (irs_dc_set_segments)
   uint32_t* d_seg_start = nullptr;  // [slot_cap + 1]
@@ -1020,6 +1023,19 @@ int irs_circuits_lift_mpc(irs_circuits* c, const uint16_t* const mask_a[3], size
 // ---------------------------------------------------------------------------
 // DistanceComparator
 // ---------------------------------------------------------------------------
+// Buffer layout of the distance capture: [0] count, then entry [cap], row
+// [cap], code [3][cap] u16, mask [3][cap] u16.
+static void set_distance_capture(irs_distance_comparator* dc, ThresholdParams& P) {
+  if (!dc->d_dist) return;
+  const size_t cap = dc->dist_cap;
+  P.dist_count = dc->d_dist;
+  P.dist_entry = dc->d_dist + 1;
+  P.dist_row = dc->d_dist + 1 + cap;
+  P.dist_code = reinterpret_cast<uint16_t*>(dc->d_dist + 1 + 2 * cap);
+  P.dist_mask = P.dist_code + 3 * cap;
+  P.dist_cap = (uint32_t)cap;
+}
+
 int irs_dc_init(irs_device_manager* dm, size_t max_queries, size_t max_db_length, size_t match_list_cap,
                 irs_distance_comparator** out) {
   CHECK(dm && out && max_queries > 0 && max_db_length > 0, IRS_ERR_INVALID, "bad arguments");
@@ -1071,7 +1087,7 @@ int irs_dc_destroy(irs_distance_comparator* dc) {
   cudaSetDevice(dc->dm->device);
   void* ps[] = {dc->bitmap, dc->self_bitmap, dc->match_list, dc->counters, dc->partial, dc->final_results,
                 dc->match_counters, dc->all_matches, dc->d_slot_valid, dc->d_slot_query,
-                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask, dc->d_take};
+                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask, dc->d_take, dc->d_dist};
   for (void* p : ps) if (p) cudaFree(p);
   delete dc;
   return IRS_OK;
@@ -1145,6 +1161,7 @@ int irs_dc_compare_threshold_open(irs_distance_comparator* dc, irs_circuits* c, 
   P.match_count = dc->counters;
   P.match_list = self_check ? nullptr : dc->match_list;
   P.match_cap = (uint32_t)dc->match_cap;
+  if (!self_check) set_distance_capture(dc, P);
   CU(launch_threshold_bitmap(P, s));
   if (slot_valid || slot_query) CU(cudaStreamSynchronize(s));  // host arrays are caller-owned
   return IRS_OK;
@@ -1221,6 +1238,7 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
   P.match_count = dc->counters;
   P.match_list = self_check ? nullptr : dc->match_list;
   P.match_cap = (uint32_t)dc->match_cap;
+  if (!self_check) set_distance_capture(dc, P);
   CU(launch_threshold_bitmap(P, s));
   return IRS_OK;
 }
@@ -1297,6 +1315,56 @@ int irs_dc_take_rows(irs_distance_comparator* dc, const uint32_t* rows, size_t n
   CU(cudaMemcpyAsync(counts, d_counts, n * 4, cudaMemcpyDeviceToHost, s));
   CU(cudaMemcpyAsync(ids, d_ids, n * kMaxMatchesLen * 4, cudaMemcpyDeviceToHost, s));
   if (!dm->host_sync) return IRS_OK;  // outputs valid once the stream passes the copies
+  CU(cudaStreamSynchronize(s));
+  return check_device_error(dm);
+}
+
+static size_t dist_bytes(size_t cap) { return (1 + 2 * cap) * 4 + 6 * cap * 2 + 16; }
+
+int irs_dc_enable_distance_capture(irs_distance_comparator* dc, size_t cap) {
+  CHECK(dc && cap > 0 && cap < (1u << 30), IRS_ERR_INVALID, "bad arguments");
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  CU(cudaStreamSynchronize(dm->streams[0]));
+  if (dc->d_dist) {
+    cudaFree(dc->d_dist);
+    dc->d_dist = nullptr;
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, dist_bytes(cap)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(IRS_ERR_NOMEM, "distance capture allocation of %zu bytes failed", dist_bytes(cap));
+  }
+  dc->d_dist = static_cast<uint32_t*>(p);
+  dc->dist_cap = cap;
+  CU(cudaMemset(dc->d_dist, 0, 4));
+  return IRS_OK;
+}
+
+int irs_dc_fetch_distances(irs_distance_comparator* dc, size_t cap, uint32_t* entry, uint32_t* row, uint16_t* code,
+                           uint16_t* mask, size_t* n, int reset) {
+  CHECK(dc && n, IRS_ERR_INVALID, "bad arguments");
+  CHECK(dc->d_dist, IRS_ERR_STATE, "distance capture not enabled");
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[0];
+  uint32_t count = 0;
+  CU(cudaMemcpyAsync(&count, dc->d_dist, 4, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  *n = count;  // may exceed the capture capacity: records beyond it were dropped
+  const size_t k = std::min<size_t>(std::min<size_t>(count, dc->dist_cap), cap);
+  const size_t dcap = dc->dist_cap;
+  if (k) {
+    CHECK(entry && row && code && mask, IRS_ERR_INVALID, "output arrays missing");
+    CU(cudaMemcpyAsync(entry, dc->d_dist + 1, k * 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(row, dc->d_dist + 1 + dcap, k * 4, cudaMemcpyDeviceToHost, s));
+    const uint16_t* dcode = reinterpret_cast<const uint16_t*>(dc->d_dist + 1 + 2 * dcap);
+    for (int p = 0; p < 3; p++) {
+      CU(cudaMemcpyAsync(code + p * cap, dcode + p * dcap, k * 2, cudaMemcpyDeviceToHost, s));
+      CU(cudaMemcpyAsync(mask + p * cap, dcode + (3 + p) * dcap, k * 2, cudaMemcpyDeviceToHost, s));
+    }
+  }
+  if (reset) CU(cudaMemsetAsync(dc->d_dist, 0, 4, s));
   CU(cudaStreamSynchronize(s));
   return check_device_error(dm);
 }

@@ -102,11 +102,36 @@ __global__ void __launch_bounds__(kThreshThreads, MIN_BLOCKS) threshold_bitmap_k
       }
     }
   };
+  uint32_t rows = 0;  // valid rows of the slot (for the distance capture)
   if (P.seg_start) {
     const uint32_t s0 = P.seg_start[slot], s1 = P.seg_start[slot + 1];
-    for (uint32_t k = s0; k < s1; k++) emit(P.seg_query[k], P.seg_mask[k], true);
+    for (uint32_t k = s0; k < s1; k++) {
+      emit(P.seg_query[k], P.seg_mask[k], true);
+      rows |= P.seg_mask[k];
+    }
   } else {
-    emit(P.slot_query ? P.slot_query[slot] : slot, P.slot_valid ? P.slot_valid[slot] : 0x7FFFFFFFu, false);
+    rows = P.slot_valid ? P.slot_valid[slot] : 0x7FFFFFFFu;
+    emit(P.slot_query ? P.slot_query[slot] : slot, rows, false);
+  }
+  // Distance capture of the per-rotation matches (openResults' match
+  // distance buffers, iris-mpc-gpu/src/dot/kernel.cu:73-106): rare, so one
+  // atomic per record.
+  if (P.dist_count && valid) {
+    uint32_t hits = opened & rows;
+    while (hits) {
+      const int r = __ffs(hits) - 1;
+      hits &= hits - 1;
+      const uint32_t pos = atomicAdd(P.dist_count, 1u);
+      if (pos < P.dist_cap) {
+        P.dist_entry[pos] = (uint32_t)m_global;
+        P.dist_row[pos] = slot * 32 + (uint32_t)r;
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+          P.dist_code[(size_t)p * P.dist_cap + pos] = code[p][r];
+          P.dist_mask[(size_t)p * P.dist_cap + pos] = mask[p][r];
+        }
+      }
+    }
   }
 }
 

@@ -37,6 +37,15 @@ struct ThresholdParams {
   uint32_t* match_count;
   uint32_t* match_list; // pairs (query, entry), optional
   uint32_t match_cap;
+  // Optional distance capture (anonymised statistics): every opened match of
+  // a valid row appends (entry, row, the three parties' code and mask dot
+  // components) at position atomicAdd(dist_count, 1) when below dist_cap.
+  uint32_t* dist_count;
+  uint32_t* dist_entry;  // [dist_cap] global DB entry
+  uint32_t* dist_row;    // [dist_cap] query row (32 * slot + row of the slot)
+  uint16_t* dist_code;   // [3][dist_cap]
+  uint16_t* dist_mask;   // [3][dist_cap]
+  uint32_t dist_cap;
 };
 
 cudaError_t launch_threshold_flat(const ThresholdParams& P, int stage, cudaStream_t stream);

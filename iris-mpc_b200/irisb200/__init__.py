@@ -66,6 +66,8 @@ _SIGS = {
     "irs_event_destroy": [_vp],
     "irs_dc_clear_rows": [_vp, _sz, _sz, _vp],
     "irs_dc_take_rows": [_vp, _vp, _sz, _sz, _i, _vp, _vp],
+    "irs_dc_enable_distance_capture": [_vp, _sz],
+    "irs_dc_fetch_distances": [_vp, _sz, _vp, _vp, _vp, _vp, C.POINTER(_sz), _i],
     "irs_dc_fetch_rows": [_vp, _sz, _sz, _vp, _sz, C.POINTER(_sz)],
     "irs_device_alloc": [_vp, _sz, C.POINTER(_vp)],
     "irs_device_free": [_vp, _vp],
@@ -574,6 +576,21 @@ class DistanceComparator:
         _check(lib().irs_dc_take_rows(self.h, _ptr(r) if r.size else None, r.size, db_len, int(clear), _ptr(counts),
                                       _ptr(ids)))
         return counts[: r.size], ids[: r.size]
+
+    def enable_distance_capture(self, cap: int) -> None:
+        _check(lib().irs_dc_enable_distance_capture(self.h, cap))
+
+    def fetch_distances(self, cap: int = 1 << 16, reset: bool = True):
+        """(entry [n], row [n], code [3][n], mask [3][n], total captured)."""
+        entry = np.zeros(cap, np.uint32)
+        row = np.zeros(cap, np.uint32)
+        code = np.zeros((3, cap), np.uint16)
+        mask = np.zeros((3, cap), np.uint16)
+        n = _sz()
+        _check(lib().irs_dc_fetch_distances(self.h, cap, _ptr(entry), _ptr(row), _ptr(code), _ptr(mask), C.byref(n),
+                                            int(reset)))
+        k = min(n.value, cap)
+        return entry[:k], row[:k], code[:, :k], mask[:, :k], n.value
 
     def take_rows_into(self, rows: np.ndarray, db_len: int, counts: np.ndarray, ids: np.ndarray,
                        clear: bool = True) -> None:
