@@ -104,12 +104,16 @@ def pack(variant_rows: list) -> Layout:
 
 
 def padded_rows(n_rows: int, cap: int) -> int:
-    """Query rows to run for `n_rows` packed rows: above 256 rows the GEMM is
-    tensor-bound and pads to a multiple of 256 (its widest tile); below, it is
-    bound by streaming the DB and keeps the fewest rows (multiple of 64)."""
-    if n_rows <= 256:
-        return -(-n_rows // 64) * 64
-    return min(-(-n_rows // 256) * 256, max(cap // 64 * 64, n_rows))
+    """Query rows to run for `n_rows` packed rows, padded for the GEMM tile the
+    library picks (gemm_block_n_for): 64 rows stay 64 (the pass streams the
+    DB), up to 768 rows pad to a multiple of 128, above to a multiple of 256."""
+    if n_rows <= 64:
+        n = 64
+    elif n_rows <= 768:
+        n = -(-n_rows // 128) * 128
+    else:
+        n = -(-n_rows // 256) * 256
+    return min(n, max(cap // 64 * 64, n_rows))
 
 
 def pad_rows(layout: Layout, cap: int) -> Layout:
