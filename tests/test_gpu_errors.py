@@ -1,0 +1,77 @@
+"""Error paths of the C ABI: every call validates its arguments on the host
+and returns a status (never aborts, never launches on bad input); the device
+stays usable afterwards.  Inputs here are rejected before any GPU work."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import irisb200
+import workload as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _raises(fn, code=-1, text=None):
+    with pytest.raises(irisb200.IrisError) as ei:
+        fn()
+    assert ei.value.code == code, str(ei.value)
+    if text:
+        assert text in str(ei.value)
+
+
+def test_rejected_inputs_leave_the_device_usable(dm):
+    e = irisb200.ShareDB(0, dm, 256, 64, 12800, W.SEEDS[0])
+    m = irisb200.ShareDB(0, dm, 256, 64, 6400, W.SEEDS[0])
+    dc = irisb200.DistanceComparator(dm, 2, 256)
+    plain = irisb200.ShareDB(0, dm, 256, 64, 12800, W.SEEDS[0], is_remote=False)
+    plain.alloc_db(256)
+    try:
+        # dot before alloc_db / query upload
+        _raises(lambda: e.dot(0, 64), -4)
+        e.alloc_db(256)
+        m.alloc_db(256)
+        _raises(lambda: e.dot(0, 64), -4, "no query")
+        # records beyond the capacity; random fill beyond the capacity
+        _raises(lambda: e.load_records(250, np.zeros((10, 12800), np.uint16)), -1, "capacity")
+        _raises(lambda: e.fill_random(1, 300), -1)
+        # row descriptors: source query out of range, rotation out of range
+        base = np.zeros((2, 12800), np.uint16)
+        _raises(lambda: e.query_upload_rows(base, np.array([(2 << 8) | 0], np.uint32)), -1, "descriptor")
+        _raises(lambda: e.query_upload_rows(base, np.array([(0 << 8) | 31], np.uint32)), -1, "descriptor")
+        # the resident pool: writes past the staging
+        _raises(lambda: e.query_put_base(64, base), -1, "pool")
+        # gathers: ids out of range, mismatched engines
+        sub = irisb200.ShareDB(0, dm, 4, 64, 12800, W.SEEDS[0])
+        sub.alloc_db(4)
+        _raises(lambda: sub.gather_records(e, np.array([300], np.uint32)), -1, "out of range")
+        _raises(lambda: sub.gather_records(m, np.array([0], np.uint32)), -1, "same party")
+        _raises(lambda: sub.gather_records(e, np.arange(5, dtype=np.uint32)), -1, "capacity")
+        sub.close()
+        # comparator: rows out of range, captures not enabled, bad segment tables
+        _raises(lambda: dc.take_rows(np.array([2], np.uint32), 10), -1, "out of range")
+        _raises(lambda: dc.fetch_distances(), -4, "not enabled")
+        _raises(lambda: dc.set_segments(np.array([1, 2], np.uint32), np.array([0], np.uint32),
+                                        np.array([1], np.uint32)), -1, "seg_start[0]")
+        _raises(lambda: dc.set_segments(np.array([0, 1], np.uint32), np.array([7], np.uint32),
+                                        np.array([1], np.uint32)), -1, "query")
+        _raises(lambda: dc.clear_rows(1, 5), -1)
+        # tile widths and batch ids
+        _raises(lambda: e.set_tile(96), -1, "tile width")
+        _raises(lambda: e.set_batch(1 << 24), -1, "2^24")
+        _raises(lambda: dm.set_batch_counter(1 << 24), -1, "2^24")
+        # the device still runs a correct pass afterwards (engine without the
+        # zero-share mask: results are the plain dots mod 2^16)
+        rows = np.random.default_rng(1).integers(0, 65536, (64, 12800), dtype=np.uint16)
+        db = np.random.default_rng(2).integers(0, 65536, (256, 12800), dtype=np.uint16)
+        plain.query_upload(rows)
+        plain.load_records(0, db)
+        plain.dot(0, 256)
+        got = plain.fetch_results(256)
+        assert dm.error_code() == 0
+        ref = (rows.astype(np.uint64) @ db.T.astype(np.uint64)) % 65536
+        assert np.array_equal(got.astype(np.uint64), ref)
+    finally:
+        dc.close()
+        for x in (e, m, plain):
+            x.close()
