@@ -64,6 +64,17 @@ def build(force: bool = False) -> None:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+def build_ref() -> bool:
+    """Compile the reference's ChaCha12 kernel into _ref/ when the reference
+    tree is present (this machine); on a machine without it the prebuilt
+    cubin, if any, is used as is.  Returns whether the cubin exists."""
+    ref = os.environ.get("IRIS_REFERENCE", "/root/reference")
+    if os.path.isdir(ref):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True)
+    return os.path.exists(REF_CHACHA_CUBIN)
+
+
+REF_CHACHA_CUBIN = os.path.join(HERE, "_ref", "chacha_ref.cubin")
 _LIB = None
 
 
