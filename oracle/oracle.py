@@ -71,10 +71,11 @@ def build_ref() -> bool:
     ref = os.environ.get("IRIS_REFERENCE", "/root/reference")
     if os.path.isdir(ref):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True)
-    return os.path.exists(REF_CHACHA_CUBIN)
+    return os.path.exists(REF_CHACHA_CUBIN) and os.path.exists(REF_DOT_CUBIN)
 
 
 REF_CHACHA_CUBIN = os.path.join(HERE, "_ref", "chacha_ref.cubin")
+REF_DOT_CUBIN = os.path.join(HERE, "_ref", "dot_ref.cubin")
 _LIB = None
 
 
