@@ -44,8 +44,8 @@ def _reference_dot(cu, fn, db, q, multiplier):
     dev = torch.device("cuda", 0)
     a0, a1 = (torch.from_numpy(x).to(dev) for x in _limbs(db))  # [M][K]
     b0, b1 = (torch.from_numpy(x).to(dev) for x in _limbs(q))   # [Q][K]
-    c = torch._int_mm(b0, a0.t().contiguous()) + 256 * (torch._int_mm(b0, a1.t().contiguous()) +
-                                                          torch._int_mm(b1, a0.t().contiguous()))
+    c = torch._int_mm(b0, a0.t()) + 256 * (torch._int_mm(b0, a1.t()) +
+                                                          torch._int_mm(b1, a0.t()))
     c = c.contiguous()  # [Q][M] i32, wrapping
     sums = [x.to(torch.int32).sum(dim=1).to(torch.int32).contiguous() for x in (a0, a1, b0, b1)]
     out = torch.zeros(Q * M, dtype=torch.int16, device=dev)
