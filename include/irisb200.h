@@ -276,6 +276,20 @@ int irs_circuits_compare_threshold_masked_many_noalloc(irs_circuits* c, const ui
 int irs_circuits_extract_msb_of_code(irs_circuits* c, const uint16_t* const code_a[3], size_t n,
                                      uint64_t* const res_a[3], uint64_t* const res_b[3], uint64_t* opened,
                                      void* stream);
+/* or_reduce_result / or_tree_on_gpu (threshold_ring/protocol.rs:2363-2515):
+ * the shared OR of all n result bits (n a multiple of 64), given every party's
+ * a-share res_a[p] (u64 words, as compare_threshold_masked_many writes them;
+ * party p's b-share is party p-1's a-share).  AND gates on each party's own
+ * view, the reference's halving tree over words, then a collapse of the last
+ * word's 32 bits.  Writes host out[0..2] = party p's a-share of the OR bit,
+ * out[3] = the opened bit.  Synchronous. */
+int irs_circuits_or_reduce(irs_circuits* c, const uint64_t* const res_a[3], size_t n, uint32_t out[4],
+                           void* stream);
+/* compare_threshold_masked_many_with_or_tree (protocol.rs:2594-2610): the
+ * threshold comparison of n elements followed by the OR tree; out as above. */
+int irs_circuits_compare_threshold_masked_many_with_or_tree(irs_circuits* c, const uint16_t* const code_a[3],
+                                                            const uint16_t* const mask_a[3], size_t n,
+                                                            uint32_t threshold_a, uint32_t out[4], void* stream);
 /* lift_mpc (protocol.rs:2041-2074): per party p, corr[p] receives two u16
  * arrays of n (party p's own component of the injected carries c1, c2);
  * sum_p mask_p - (sum corr1 << 16) - (sum corr2 << 17) = mask in Z_2^32. */

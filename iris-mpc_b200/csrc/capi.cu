@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/irisb200.h"
+#include "or_tree.h"
 #include "common.cuh"
 #include "gemm_limb.h"
 #include "internal.h"
@@ -985,6 +986,83 @@ int irs_circuits_compare_threshold_masked_many(irs_circuits* c, const uint16_t* 
                                                uint64_t* const res_a[3], uint64_t* const res_b[3], uint64_t* opened,
                                                void* stream) {
   return run_flat(c, code_a, mask_a, n, threshold_a, res_a, res_b, opened, kStageFull, stream);
+}
+
+// The shared OR of the bit vector whose components are comp[p * n_words + w]
+// (party p's a-share), into host out[4]: the three components and the opened
+// bit.  Synchronous.
+static int run_or_tree(irs_circuits* c, const uint32_t* comp, size_t n_words, uint32_t* out, cudaStream_t s) {
+  irs_device_manager* dm = c->dm;
+  OrTreeParams P;
+  memset(&P, 0, sizeof P);
+  for (int p = 0; p < 3; p++) P.key[p] = c->keys[p];
+  P.nonce = nonce_of(kDomOrTree, (uint32_t)dm->device);
+  P.batch = c->batch;
+  P.batch_dev = c->batch_from_device ? dm->d_batch : nullptr;
+  void* p;
+  int rc = pool_alloc(dm, 0, (6 * n_words + 4) * 4, &p);
+  if (rc) return rc;
+  uint32_t* scratch = static_cast<uint32_t*>(p);
+  uint32_t* out4 = scratch + 6 * n_words;
+  cudaError_t e = launch_or_tree(P, comp, n_words, scratch, out4, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, out4, 16, cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(scratch, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(IRS_ERR_CUDA, "or tree: %s", cudaGetErrorString(e));
+  return check_device_error(dm);
+}
+
+int irs_circuits_or_reduce(irs_circuits* c, const uint64_t* const res_a[3], size_t n, uint32_t out[4], void* stream) {
+  CHECK(c && res_a && out, IRS_ERR_INVALID, "bad arguments");
+  CHECK(n > 0 && n % 64 == 0, IRS_ERR_INVALID, "n = %zu must be a positive multiple of 64", n);
+  for (int p = 0; p < 3; p++) CHECK(res_a[p], IRS_ERR_INVALID, "share pointer missing");
+  irs_device_manager* dm = c->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = party_stream(dm, 0, stream);
+  const size_t n_words = n / 32;
+  // gather the three a-shares (u64 words = pairs of u32 words) into one [3][n_words] vector
+  void* p;
+  int rc = pool_alloc(dm, 0, 3 * n_words * 4, &p);
+  if (rc) return rc;
+  uint32_t* comp = static_cast<uint32_t*>(p);
+  cudaError_t e = cudaSuccess;
+  for (int q = 0; q < 3 && e == cudaSuccess; q++)
+    e = cudaMemcpyAsync(comp + q * n_words, res_a[q], n_words * 4, cudaMemcpyDeviceToDevice, s);
+  rc = e == cudaSuccess ? run_or_tree(c, comp, n_words, out, s) : fail(IRS_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
+  cudaFreeAsync(comp, s);
+  return rc;
+}
+
+int irs_circuits_compare_threshold_masked_many_with_or_tree(irs_circuits* c, const uint16_t* const code_a[3],
+                                                            const uint16_t* const mask_a[3], size_t n,
+                                                            uint32_t threshold_a, uint32_t out[4], void* stream) {
+  CHECK(c && code_a && mask_a && out, IRS_ERR_INVALID, "bad arguments");
+  CHECK(n > 0 && n % 64 == 0, IRS_ERR_INVALID, "n = %zu must be a positive multiple of 64", n);
+  for (int p = 0; p < 3; p++) {
+    CHECK(code_a[p] && mask_a[p], IRS_ERR_INVALID, "share pointer missing");
+    CHECK(((uintptr_t)code_a[p] & 15) == 0 && ((uintptr_t)mask_a[p] & 15) == 0, IRS_ERR_INVALID,
+          "share pointers must be 16-byte aligned");
+  }
+  irs_device_manager* dm = c->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = party_stream(dm, 0, stream);
+  ThresholdParams P;
+  base_params(c, P);
+  for (int p = 0; p < 3; p++) {
+    P.code[p] = code_a[p];
+    P.mask[p] = mask_a[p];
+  }
+  P.threshold_a = threshold_a;
+  P.n_words = n / 32;
+  void* p;
+  int rc = pool_alloc(dm, 0, 3 * P.n_words * 4, &p);
+  if (rc) return rc;
+  P.res_comp = static_cast<uint32_t*>(p);
+  cudaError_t e = launch_threshold_flat(P, kStageFull, s);
+  rc = e == cudaSuccess ? run_or_tree(c, P.res_comp, P.n_words, out, s)
+                        : fail(IRS_ERR_CUDA, "threshold launch: %s", cudaGetErrorString(e));
+  cudaFreeAsync(P.res_comp, s);
+  return rc;
 }
 
 int irs_circuits_extract_msb_of_code(irs_circuits* c, const uint16_t* const code_a[3], size_t n,

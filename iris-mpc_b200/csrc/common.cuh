@@ -20,6 +20,7 @@ constexpr int kSlotRows = 32;       // query rows reserved per query iris (31 ro
 constexpr uint32_t kDomCodeDot = 1;
 constexpr uint32_t kDomMaskDot = 2;
 constexpr uint32_t kDomCircuit = 3;
+constexpr uint32_t kDomOrTree = 4;
 // Circuit keystream: 8 blocks (128 words) per 32-element word and stream.
 constexpr int kCircuitBlocksPerWord = 8;
 

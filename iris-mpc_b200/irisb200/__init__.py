@@ -119,6 +119,8 @@ _SIGS = {
     "irs_circuits_compare_threshold_masked_many_noalloc": [_vp, _vp, _vp, _sz, _u32, _vp, _vp, _vp, _vp],
     "irs_circuits_extract_msb_of_code": [_vp, _vp, _sz, _vp, _vp, _vp, _vp],
     "irs_circuits_lift_mpc": [_vp, _vp, _sz, _vp, _vp],
+    "irs_circuits_or_reduce": [_vp, _vp, _sz, _vp, _vp],
+    "irs_circuits_compare_threshold_masked_many_with_or_tree": [_vp, _vp, _vp, _sz, _u32, _vp, _vp],
     "irs_dc_init": [_vp, _sz, _sz, _sz, C.POINTER(_vp)],
     "irs_dc_destroy": [_vp],
     "irs_dc_reset": [_vp, _vp],
@@ -518,6 +520,18 @@ class Circuits:
         _check(lib().irs_circuits_extract_msb_of_code(
             self.h, _ptr3(code_a), n, _ptr3(res_a) if res_a else None, _ptr3(res_b) if res_b else None,
             opened.ptr if opened else None, stream))
+
+    def or_reduce(self, res_a, n: int, stream=None):
+        """(party a-shares [3] of the OR bit, opened bit) of n result bits."""
+        out = np.zeros(4, np.uint32)
+        _check(lib().irs_circuits_or_reduce(self.h, _ptr3(res_a), n, _ptr(out), stream))
+        return out[:3].copy(), int(out[3])
+
+    def compare_threshold_masked_many_with_or_tree(self, code_a, mask_a, n: int, threshold_a: int, stream=None):
+        out = np.zeros(4, np.uint32)
+        _check(lib().irs_circuits_compare_threshold_masked_many_with_or_tree(
+            self.h, _ptr3(code_a), _ptr3(mask_a), n, threshold_a, _ptr(out), stream))
+        return out[:3].copy(), int(out[3])
 
     def lift_mpc(self, mask_a, n: int, corr, stream=None) -> None:
         _check(lib().irs_circuits_lift_mpc(self.h, _ptr3(mask_a), n, _ptr3(corr), stream))

@@ -630,6 +630,56 @@ void orc_threshold_words(const u16 *const *code, const u16 *const *mask, long n_
 
 /* The match predicate of the plaintext values (threshold.rs:110-124):
  * bit31((mask * A - code * 2^16 - 1) mod 2^32). */
+/* MPC OR tree (or_reduce_result / or_tree_on_gpu, protocol.rs:2363-2515):
+ * comp [3][n] = the three components (party p's a-shares) of a bit vector in
+ * u32 words.  Each level ORs word i with word i + num (num = half, rounded
+ * down) and moves an odd last word down; the last word's 32 bits are then
+ * collapsed with shifts 16, 8, 4, 2, 1.  OR(x, y) = x ^ y ^ AND(x, y); the AND
+ * gate of level L, index i takes word 0 of the ChaCha12 block at counter
+ * (batch << 40) | (L << 34) | i of each party's stream (nonce domain 4), party
+ * p masking with k_p ^ k_{p-1}.  out[0..2] = components of the OR bit, out[3]
+ * = the opened bit.  comp is overwritten. */
+#define DOM_OR_TREE 4u
+static void or_gate(u32 x[3], const u32 y[3], const u32 *keys, u32 dev, u64 batch, u64 gate) {
+    u32 k[3], blk[16], z[3];
+    for (int s = 0; s < 3; s++) {
+        orc_chacha_block(keys + 8 * s, counter_of(batch, gate), nonce_of(DOM_OR_TREE, dev), 12, blk);
+        k[s] = blk[0];
+    }
+    for (int p = 0; p < 3; p++) {
+        int q = (p + 2) % 3;
+        z[p] = (x[p] & y[p]) ^ (x[q] & y[p]) ^ (x[p] & y[q]) ^ (k[p] ^ k[q]);
+    }
+    for (int p = 0; p < 3; p++) x[p] = x[p] ^ y[p] ^ z[p];
+}
+
+void orc_or_tree(u32 *comp, long n, const u32 *keys, u32 dev, u64 batch, u32 *out) {
+    long num = n;
+    u64 level = 1;
+    while (num > 1) {
+        long odd = num & 1;
+        num >>= 1;
+        for (long i = 0; i < num; i++) {
+            u32 x[3], y[3];
+            for (int p = 0; p < 3; p++) { x[p] = comp[p * n + i]; y[p] = comp[p * n + i + num]; }
+            or_gate(x, y, keys, dev, batch, (level << 34) | (u64)i);
+            for (int p = 0; p < 3; p++) comp[p * n + i] = x[p];
+        }
+        if (odd)
+            for (int p = 0; p < 3; p++) comp[p * n + num] = comp[p * n + 2 * num];
+        num += odd;
+        level++;
+    }
+    u32 x[3] = {comp[0], comp[n], comp[2 * n]};
+    int j = 0;
+    for (int sh = 16; sh >= 1; sh >>= 1, j++) {
+        u32 y[3] = {x[0] >> sh, x[1] >> sh, x[2] >> sh};
+        or_gate(x, y, keys, dev, batch, (u64)(40 + j) << 34);
+    }
+    for (int p = 0; p < 3; p++) out[p] = x[p] & 1u;
+    out[3] = (x[0] ^ x[1] ^ x[2]) & 1u;
+}
+
 int orc_match_predicate(u16 code, u16 mask, u32 threshold_a) {
     u32 r = (u32)mask * threshold_a - ((u32)code << 16) - 1u;
     return (int)(r >> 31);

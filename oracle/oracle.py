@@ -110,6 +110,7 @@ def lib():
     L.orc_dot_u16.argtypes = [_u16p, C.c_int, _u16p, C.c_long, C.c_int, _u16p]
     L.orc_chacha_block.argtypes = [_u32p, C.c_uint64, C.c_uint64, C.c_int, _u32p]
     L.orc_chacha_fill.argtypes = [_u32p, C.c_uint64, C.c_uint64, C.c_int, _u32p, C.c_long]
+    L.orc_or_tree.argtypes = [_u32p, C.c_long, _u32p, C.c_uint32, C.c_uint64, _u32p]
     L.orc_mask_dot_shares.argtypes = [_u16p, C.c_long, C.c_long, C.c_int, C.c_uint16, _u32p, _u32p,
                                       C.c_uint32, C.c_uint32, C.c_uint64]
     P = C.POINTER(C.c_void_p)
@@ -361,6 +362,17 @@ def threshold_words(code_parts, mask_parts, threshold_a: int, keys, dev: int = 0
         out["lift_x"] = lift_x
         out["corr"] = corr
     return out
+
+
+def or_tree(comp, keys, dev: int = 0, batch: int = 0):
+    """MPC OR of all bits of a shared u32 word vector (orc_or_tree): comp =
+    three u32 arrays (component p = party p's a-share).  Returns (components
+    [3] of the OR bit, opened bit)."""
+    c = np.ascontiguousarray(np.stack([np.asarray(x, np.uint32) for x in comp]))
+    keys_arr = np.ascontiguousarray(np.array(keys, np.uint32).reshape(3, 8))
+    out = np.zeros(4, np.uint32)
+    lib().orc_or_tree(c.reshape(-1), c.shape[1], keys_arr.reshape(-1), dev, batch, out)
+    return out[:3].copy(), int(out[3])
 
 
 def match_predicate(code, mask, threshold_a: int) -> np.ndarray:

@@ -230,3 +230,20 @@ def test_lift_oracle(oracle):
     assert set(np.unique(c1)) <= {0, 1} and set(np.unique(c2)) <= {0, 1}
     rec = (lx - (c1 << 16) - (c2 << 17)) % (1 << 32)
     assert np.array_equal(rec, mask.astype(np.uint64))
+
+
+def test_or_tree_oracle(oracle):
+    """The oracle's MPC OR tree opens to the OR of the shared bits, for odd and
+    even word counts and a single set bit anywhere (threshold_and_or_tree.rs)."""
+    rng = np.random.default_rng(9)
+    keys = [[0] * 8, [1] * 8, [2] * 8]
+    for n in (1, 2, 3, 7, 64, 101):
+        for bit in (None, 0, 32 * n - 1, int(rng.integers(0, 32 * n))):
+            plain = np.zeros(n, np.uint32)
+            if bit is not None:
+                plain[bit // 32] = np.uint32(1 << (bit % 32))
+            a = rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32)
+            b = rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32)
+            comps, opened = oracle.or_tree([a, b, a ^ b ^ plain], keys)
+            assert opened == int(bit is not None), (n, bit)
+            assert int(comps[0] ^ comps[1] ^ comps[2]) == opened
