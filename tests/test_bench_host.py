@@ -1,0 +1,50 @@
+"""Host-side pieces of the benchmark (no GPU): the request mix of the batched
+and serving workloads, the comparison count, and the latency/throughput
+summary of an open-loop run."""
+from __future__ import annotations
+
+import numpy as np
+
+import bench
+from irisb200.batched import Request
+from irisb200.serving import Completion
+
+
+def test_request_mix_proportions():
+    z = np.zeros((3, 16, 1), np.uint16)
+    planted = {0: (5, 0), 10: (77, 3)}
+    reqs = bench.request_mix(4000, z, z, planted, 1000, seed=1, p_append=0.01)
+    kinds = [r.kind for r in reqs]
+    n_app = kinds.count("append")
+    n_re = kinds.count("reauth")
+    n_u = kinds.count("uniqueness")
+    assert 20 <= n_app <= 70
+    assert 0.15 < n_re / (n_re + n_u) < 0.25
+    rots = [r.n_rot for r in reqs if r.kind != "append"]
+    assert set(rots) == {1, 16, 31}
+    mir = np.mean([r.mirrored for r in reqs if r.kind != "append"])
+    assert 0.45 < mir < 0.55
+    for i, r in enumerate(reqs):
+        if r.kind == "reauth":
+            assert 0 <= r.target < 1000
+            if i % 16 in planted:
+                assert r.target == planted[i % 16][0]
+    # seeded: the same seed gives the same mix
+    again = bench.request_mix(4000, z, z, planted, 1000, seed=1, p_append=0.01)
+    assert [(r.kind, r.n_rot, r.mirrored, r.target) for r in again] == \
+        [(r.kind, r.n_rot, r.mirrored, r.target) for r in reqs]
+
+
+def test_comparisons_and_latency_summary():
+    u = Request(code=None, mask=None, n_rot=16, mirrored=True)
+    r = Request(code=None, mask=None, kind="reauth", target=3)
+    a = Request(code=None, mask=None, kind="append")
+    assert bench.comparisons_of(u, 1000) == 2000
+    assert bench.comparisons_of(r, 1000) == 1
+    reqs = [u, r, a, u]
+    comps = [Completion(0, 10.0, 10.1, None), Completion(1, 10.0, 10.3, None), Completion(2, 10.0, 10.0, None),
+             Completion(3, 10.5, 11.0, None)]
+    st = bench._latency_stats(comps, reqs, 10.0, [1000, 1000, 1001, 1001])
+    assert st["completed"] == 4
+    assert abs(st["p50_ms"] - 300.0) < 1e-6 and abs(st["max_ms"] - 500.0) < 1e-6
+    assert abs(st["comparisons_per_s"] - (2000 + 1 + 2002) / 1.0) < 1e-6
