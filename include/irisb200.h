@@ -65,7 +65,9 @@ int irs_device_manager_synchronize(irs_device_manager* dm);
 /* Device error word: 0, or the code of the first bounded wait that expired. */
 int irs_device_manager_error(irs_device_manager* dm, int* code);
 int irs_device_manager_clear_error(irs_device_manager* dm);
-/* Device-resident batch counter: engines and circuits switched to it with
+/* Device-resident batch counter (the reference advances host-side ChaCha
+ * counters instead, ChachaCommon::advance_counter, rng/chacha.rs:32-36):
+ * engines and circuits switched to it with
  * irs_sharedb_use_batch_counter / irs_circuits_use_batch_counter read their
  * ChaCha batch id from device memory at run time, so a captured graph can be
  * replayed for every batch with a fresh counter (set here, outside capture). */
@@ -76,7 +78,8 @@ int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_
 int irs_device_manager_advance_batch_counter(irs_device_manager* dm, void* stream);
 /* Number of SMs the persistent kernels size their grids to. */
 int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
-/* Host synchronisation of the calls that take host buffers (default on).
+/* Host synchronisation of the calls that take host buffers (default on; no
+ * counterpart in the reference, whose calls are stream-ordered cudarc copies).
  * With it off, irs_sharedb_query_put_base, irs_sharedb_query_expand_rows,
  * irs_sharedb_query_upload_rows, irs_sharedb_gather_records,
  * irs_dc_set_segments and irs_dc_take_rows return as soon as their copies and
@@ -86,14 +89,16 @@ int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
  * party-0 stream has completed (device errors: irs_device_manager_error).  A
  * serving loop uses this to prepare and launch step k+1 while step k runs. */
 int irs_device_manager_set_host_sync(irs_device_manager* dm, int on);
-/* CUDA events for the asynchronous mode (cudaEventDisableTiming). */
+/* CUDA events for the asynchronous mode (cudaEventDisableTiming); the
+ * reference uses raw CUevents through cudarc (device_manager.rs). */
 int irs_event_create(void** ev);
 int irs_event_record(void* ev, void* stream);
 int irs_event_synchronize(void* ev);
 /* *done = 1 when the work before the event has completed, else 0. */
 int irs_event_query(void* ev, int* done);
 int irs_event_destroy(void* ev);
-/* Free and total device memory (cudaMemGetInfo), for admission by free HBM. */
+/* Free and total device memory (cudaMemGetInfo), for admission by free HBM
+ * (no counterpart: the reference sizes its batches statically). */
 int irs_device_manager_mem_info(irs_device_manager* dm, size_t* free_bytes, size_t* total_bytes);
 
 /* Plain device memory helpers for callers that stage their own buffers. */
@@ -145,7 +150,8 @@ int irs_sharedb_synth_db(irs_sharedb* const code_engines[3], irs_sharedb* const 
 /* Records 0..n-1 of one engine filled with seeded uniform limb bytes (a
  * single-engine benchmark DB: the GEMM sweep of matmul.rs has no encoding). */
 int irs_sharedb_fill_random(irs_sharedb* db, uint64_t seed, size_t n);
-/* Seeded uniform bytes in a device buffer (8-byte aligned, bytes % 8 == 0). */
+/* Seeded uniform bytes in a device buffer (8-byte aligned, bytes % 8 == 0);
+ * benchmark inputs, no counterpart in the reference. */
 int irs_device_fill_random(void* ptr, size_t bytes, uint64_t seed, void* stream);
 
 /* preprocess_iris_code_query_share / preprocess_mask_code_query_share
@@ -184,13 +190,13 @@ int irs_sharedb_query_upload_slots(irs_sharedb* db, const uint16_t* base, size_t
 /* Uploads preprocessed base queries [n_base][code_length] and fills query row
  * r with row_desc[r] = (src << 8) | rotation (rotation 0..30 of base query src,
  * 15 = centre), 0xFFFFFFFF = zero row.  Packs queries with any rotation count
- * densely (the batched launch of uneven requests). */
+ * densely (the batched launch of uneven requests).  No counterpart in the
+ * reference, which gives every query a block of 31 rotation rows
+ * (htod_transfer_query, device_manager.rs:159-212). */
 int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t n_base, const uint32_t* row_desc,
                                   size_t n_rows);
-/* prefetch_subset (share_db.rs:344-407), device to device: copies DB records
- * ids[k] of `src` into records k of `dst` (same party and code length) and
- * sets dst's length to n.  Used for reauth targets and subset re-checks. */
-/* Resident base-query pool for a serving loop: writes preprocessed base
+/* Resident base-query pool for a serving loop (no counterpart in the
+ * reference, whose actor uploads every batch whole): writes preprocessed base
  * queries [first, first + n) of the pool (the query staging area) without
  * touching the others, so a request admitted while others are in flight costs
  * one upload of its own shares. */
@@ -198,13 +204,19 @@ int irs_sharedb_query_put_base(irs_sharedb* db, size_t first, size_t n, const ui
 /* irs_sharedb_query_upload_rows over the resident pool [0, n_base): rebuilds
  * the query rows from the row table alone. */
 int irs_sharedb_query_expand_rows(irs_sharedb* db, size_t n_base, const uint32_t* row_desc, size_t n_rows);
+/* prefetch_subset (share_db.rs:344-407), device to device: copies DB records
+ * ids[k] of `src` into records k of `dst` (same party and code length) and
+ * sets dst's length to n.  Used for reauth targets and subset re-checks. */
 int irs_sharedb_gather_records(irs_sharedb* dst, irs_sharedb* src, const uint32_t* ids, size_t n);
 /* mirrored_code / mirrored_mask (galois_engine.rs:218-225,520-543) of a
  * (preprocessed or raw) query share, in place; flip_imaginary = 1 for codes. */
 int irs_mirror_query_share(uint16_t* coefs, size_t n, int flip_imaginary);
 /* Tile width of the dot kernel along the query rows: 64, 128 or 256, or 0 for
- * the widest that divides the padded row count (the batch autotuner's knob).
- * The padded row count of a batch is its uploaded rows rounded up to 64. */
+ * the library's choice (the batch autotuner's knob; no counterpart in the
+ * reference, where cuBLAS picks its own tiles).  The padded row count of a
+ * batch is its uploaded rows rounded up to 64, and further to 128 (up to 768
+ * rows) or 256 (above) when the query capacity allows; the extra rows are zero.
+ * Default: the 128-row tile up to 768 padded rows, else the 256-row tile. */
 int irs_sharedb_set_tile(irs_sharedb* db, int block_n);
 int irs_sharedb_use_batch_counter(irs_sharedb* db, int on);
 /* Starts a new batch: the zero-share mask and circuit keystreams are drawn at
@@ -321,7 +333,8 @@ int irs_dc_compare_threshold_open(irs_distance_comparator* dc, irs_circuits* c, 
                                   irs_sharedb* const mask_engines[3], size_t offset, size_t len, size_t n_slots,
                                   const uint32_t* slot_valid, const uint32_t* slot_query, uint32_t threshold_a,
                                   int self_check, void* stream);
-/* Segment table for packed query rows: slot s (32 rows) holds segments
+/* Segment table for packed query rows (no counterpart in the reference, one
+ * query per 31 rows there): slot s (32 rows) holds segments
  * seg_start[s] .. seg_start[s+1]-1; segment k ORs the opened bits of rows
  * seg_mask[k] into bitmap row seg_query[k].  Copied to the device once, so the
  * prepared call below can run inside a captured CUDA graph. */
@@ -356,7 +369,7 @@ int irs_dc_enable_distance_capture(irs_distance_comparator* dc, size_t cap);
 int irs_dc_fetch_distances(irs_distance_comparator* dc, size_t cap, uint32_t* entry, uint32_t* row, uint16_t* code,
                            uint16_t* mask, size_t* n, int reset);
 /* Clears bitmap rows [first, first + n) (a query row reused by the serving
- * loop for a new request). */
+ * loop for a new request; no counterpart in the reference). */
 int irs_dc_clear_rows(irs_distance_comparator* dc, size_t first, size_t n, void* stream);
 /* Bitmap rows [first, first + n) in the internal layout: u32 words
  * [n][row_words], bit j of word w = entry 32w + j; *row_words receives the
@@ -389,7 +402,8 @@ int irs_dc_fetch_final_results(irs_distance_comparator* dc, size_t n_queries, ui
                                uint32_t* match_counters, uint32_t* all_matches);
 
 /* ------------------------------------------------------------------------ */
-/* CUDA graphs of a batch's device work (party 0's stream).                  */
+/* CUDA graphs of a batch's device work (party 0's stream).  No counterpart */
+/* in the reference, which launches every kernel through cudarc.            */
 /* Between begin and end, the library keeps all launches on the capturing    */
 /* stream (no cross-party event waits); calls that synchronise the host fail */
 /* with the CUDA capture error.                                              */
