@@ -363,6 +363,11 @@ int irs_dc_take_rows(irs_distance_comparator* dc, const uint32_t* rows, size_t n
  * records (further matches are counted, not stored).  Run it on the prefilter
  * pass (IRS_THRESHOLD_ANON_STATS_A) as the reference does. */
 int irs_dc_enable_distance_capture(irs_distance_comparator* dc, size_t cap);
+/* Pairs (bitmap row query[i], DB entry entry[i]) whose distances are captured
+ * for every valid query row whether or not they match (openResults'
+ * anon_stats_idx, kernel.cu:73-86: the reauth targets); n <= 256, replaces the
+ * previous list, n = 0 clears it.  Needs the capture enabled. */
+int irs_dc_set_forced_distances(irs_distance_comparator* dc, const uint32_t* query, const uint32_t* entry, size_t n);
 /* Copies up to `cap` captured records: entry [cap], row [cap], code [3][cap],
  * mask [3][cap] (component p at p * cap); *n = records captured so far
  * (possibly above the capture capacity).  reset != 0 empties the capture. */

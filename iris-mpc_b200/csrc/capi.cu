@@ -126,6 +126,8 @@ struct irs_distance_comparator {
   // distance capture (irs_dc_enable_distance_capture): count, entry, row, code [3], mask [3]
   uint32_t* d_dist = nullptr;
   size_t dist_cap = 0;
+  uint32_t* d_forced = nullptr;  // forced records: query [256], entry [256]
+  uint32_t n_forced = 0;
   size_t slot_cap = 0;
   // segment table (irs_dc_set_segments)
   uint32_t* d_seg_start = nullptr;  // [slot_cap + 1]
@@ -1113,6 +1115,8 @@ int irs_circuits_lift_mpc(irs_circuits* c, const uint16_t* const mask_a[3], size
 // ---------------------------------------------------------------------------
 // DistanceComparator
 // ---------------------------------------------------------------------------
+constexpr uint32_t kMaxForced = 256;
+
 // Buffer layout of the distance capture: [0] count, then entry [cap], row
 // [cap], code [3][cap] u16, mask [3][cap] u16.
 static void set_distance_capture(irs_distance_comparator* dc, ThresholdParams& P) {
@@ -1124,6 +1128,11 @@ static void set_distance_capture(irs_distance_comparator* dc, ThresholdParams& P
   P.dist_code = reinterpret_cast<uint16_t*>(dc->d_dist + 1 + 2 * cap);
   P.dist_mask = P.dist_code + 3 * cap;
   P.dist_cap = (uint32_t)cap;
+  if (dc->d_forced && dc->n_forced) {
+    P.forced_query = dc->d_forced;
+    P.forced_entry = dc->d_forced + kMaxForced;
+    P.n_forced = dc->n_forced;
+  }
 }
 
 int irs_dc_init(irs_device_manager* dm, size_t max_queries, size_t max_db_length, size_t match_list_cap,
@@ -1177,7 +1186,7 @@ int irs_dc_destroy(irs_distance_comparator* dc) {
   cudaSetDevice(dc->dm->device);
   void* ps[] = {dc->bitmap, dc->self_bitmap, dc->match_list, dc->counters, dc->partial, dc->final_results,
                 dc->match_counters, dc->all_matches, dc->d_slot_valid, dc->d_slot_query,
-                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask, dc->d_take, dc->d_dist};
+                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask, dc->d_take, dc->d_dist, dc->d_forced};
   for (void* p : ps) if (p) cudaFree(p);
   delete dc;
   return IRS_OK;
@@ -1428,6 +1437,32 @@ int irs_dc_enable_distance_capture(irs_distance_comparator* dc, size_t cap) {
   dc->d_dist = static_cast<uint32_t*>(p);
   dc->dist_cap = cap;
   CU(cudaMemset(dc->d_dist, 0, 4));
+  return IRS_OK;
+}
+
+int irs_dc_set_forced_distances(irs_distance_comparator* dc, const uint32_t* query, const uint32_t* entry, size_t n) {
+  CHECK(dc && (n == 0 || (query && entry)), IRS_ERR_INVALID, "bad arguments");
+  CHECK(dc->d_dist, IRS_ERR_STATE, "distance capture not enabled");
+  CHECK(n <= kMaxForced, IRS_ERR_INVALID, "%zu forced pairs exceed %u", n, kMaxForced);
+  for (size_t i = 0; i < n; i++)
+    CHECK(query[i] < dc->max_queries && entry[i] < dc->max_db, IRS_ERR_INVALID, "forced pair %zu out of range", i);
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[0];
+  if (!dc->d_forced) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, 2 * kMaxForced * 4) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(IRS_ERR_NOMEM, "forced-pair table allocation failed");
+    }
+    dc->d_forced = static_cast<uint32_t*>(p);
+  }
+  if (n) {
+    CU(cudaMemcpyAsync(dc->d_forced, query, n * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(dc->d_forced + kMaxForced, entry, n * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaStreamSynchronize(s));  // caller-owned host memory
+  }
+  dc->n_forced = (uint32_t)n;
   return IRS_OK;
 }
 

@@ -118,6 +118,16 @@ __global__ void __launch_bounds__(kThreshThreads, MIN_BLOCKS) threshold_bitmap_k
   // atomic per record.
   if (P.dist_count && valid) {
     uint32_t hits = opened & rows;
+    // forced pairs: every valid row of a listed (query, entry) is recorded
+    for (uint32_t j = 0; j < P.n_forced; j++) {
+      if (P.forced_entry[j] != (uint32_t)m_global) continue;
+      if (P.seg_start) {
+        for (uint32_t k = P.seg_start[slot]; k < P.seg_start[slot + 1]; k++)
+          if (P.seg_query[k] == P.forced_query[j]) hits |= P.seg_mask[k];
+      } else if ((P.slot_query ? P.slot_query[slot] : slot) == P.forced_query[j]) {
+        hits |= rows;
+      }
+    }
     while (hits) {
       const int r = __ffs(hits) - 1;
       hits &= hits - 1;

@@ -46,6 +46,11 @@ struct ThresholdParams {
   uint16_t* dist_code;   // [3][dist_cap]
   uint16_t* dist_mask;   // [3][dist_cap]
   uint32_t dist_cap;
+  // (query, entry) pairs recorded for every valid row whether or not they
+  // match (the reference's anon_stats_idx: reauth targets), n_forced <= 256
+  const uint32_t* forced_query;
+  const uint32_t* forced_entry;
+  uint32_t n_forced;
 };
 
 cudaError_t launch_threshold_flat(const ThresholdParams& P, int stage, cudaStream_t stream);

@@ -67,6 +67,7 @@ _SIGS = {
     "irs_dc_clear_rows": [_vp, _sz, _sz, _vp],
     "irs_dc_take_rows": [_vp, _vp, _sz, _sz, _i, _vp, _vp],
     "irs_dc_enable_distance_capture": [_vp, _sz],
+    "irs_dc_set_forced_distances": [_vp, _vp, _vp, _sz],
     "irs_dc_fetch_distances": [_vp, _sz, _vp, _vp, _vp, _vp, C.POINTER(_sz), _i],
     "irs_dc_fetch_rows": [_vp, _sz, _sz, _vp, _sz, C.POINTER(_sz)],
     "irs_device_alloc": [_vp, _sz, C.POINTER(_vp)],
@@ -593,6 +594,13 @@ class DistanceComparator:
 
     def enable_distance_capture(self, cap: int) -> None:
         _check(lib().irs_dc_enable_distance_capture(self.h, cap))
+
+    def set_forced_distances(self, pairs) -> None:
+        """(query, entry) pairs captured on every valid row, match or not."""
+        q = np.ascontiguousarray([p[0] for p in pairs], np.uint32)
+        e = np.ascontiguousarray([p[1] for p in pairs], np.uint32)
+        _check(lib().irs_dc_set_forced_distances(self.h, _ptr(q) if q.size else None, _ptr(e) if e.size else None,
+                                                 q.size))
 
     def fetch_distances(self, cap: int = 1 << 16, reset: bool = True):
         """(entry [n], row [n], code [3][n], mask [3][n], total captured)."""
