@@ -60,6 +60,15 @@ class Result:
     reauth_mirror_match: bool | None = None
 
 
+def full_face_mirror_attack(request: Request, result: Result) -> bool:
+    """Full-face mirror attack detection (iris-mpc-gpu/src/server/actor.rs:
+    1316-1336): a uniqueness request whose normal orientation matches no DB
+    entry while its mirrored orientation matches one.  Other request kinds,
+    and requests without a mirrored orientation, are never flagged."""
+    return (request.kind == "uniqueness" and request.mirrored and not result.matches
+            and bool(result.mirror_matches))
+
+
 @dataclass
 class Layout:
     """Dense packing of the variants' rows into 32-row words."""

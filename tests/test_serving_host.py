@@ -175,3 +175,14 @@ def test_serve_loop_admission_and_append_barrier(monkeypatch):
     # every uniqueness request visited all 4 chunks of its DB snapshot
     assert s.steps >= 8 and not s.flight and sorted(s.free_variants) == list(range(16))
     assert s.slot_occ == [0, 0, 0, 0]
+
+
+def test_full_face_mirror_attack_rule():
+    from irisb200.batched import Request, Result, full_face_mirror_attack
+    u = Request(code=None, mask=None, mirrored=True)
+    assert full_face_mirror_attack(u, Result(matches=[], mirror_matches=[7]))
+    assert not full_face_mirror_attack(u, Result(matches=[3], mirror_matches=[7]))   # both matched
+    assert not full_face_mirror_attack(u, Result(matches=[], mirror_matches=[]))
+    r = Request(code=None, mask=None, mirrored=True, kind="reauth", target=1)
+    assert not full_face_mirror_attack(r, Result(matches=[], mirror_matches=[7]))
+    assert not full_face_mirror_attack(Request(code=None, mask=None), Result(matches=[], mirror_matches=[7]))
