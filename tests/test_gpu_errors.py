@@ -76,3 +76,38 @@ def test_rejected_inputs_leave_the_device_usable(dm):
         dc.close()
         for x in (e, m, plain):
             x.close()
+
+
+def test_empty_inputs_are_no_ops(dm):
+    """Zero-length work is accepted and changes nothing: a dot and a
+    comparison over no entries, a compaction of no rows, an empty subset
+    gather, and the final results of a batch that matched nothing."""
+    ce = [irisb200.ShareDB(p, dm, 128, 64, 12800, W.SEEDS[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, 128, 64, 6400, W.SEEDS[p]) for p in range(3)]
+    c = irisb200.Circuits(dm, W.SEEDS)
+    dc = irisb200.DistanceComparator(dm, 2, 128)
+    try:
+        slots = [(0, 0, 31, 0), (0, 0, 31, 1)]
+        for p in range(3):
+            ce[p].alloc_db(128)
+            me[p].alloc_db(128)
+            ce[p].query_upload_slots(np.zeros((1, 12800), np.uint16), slots)
+            me[p].query_upload_slots(np.zeros((1, 6400), np.uint16), slots)
+        irisb200.dot_many(ce + me, [1, 1, 1, 2, 2, 2], 0, 0)
+        dc.compare_threshold_open(c, ce, me, 0, 0, 2, 16384)
+        counts, ids = dc.take_rows(np.zeros(0, np.uint32), 0)
+        assert counts.size == 0 and ids.shape[0] == 0
+        sub = irisb200.ShareDB(0, dm, 4, 64, 12800, W.SEEDS[0])
+        sub.alloc_db(4)
+        sub.gather_records(ce[0], np.zeros(0, np.uint32))
+        assert sub.db_len() == 0
+        sub.close()
+        dc.join_db_matches(2, 0)
+        final, counters, _ = dc.fetch_final_results(2)
+        assert (final == 0xFFFFFFFF).all() and (counters == 0).all()
+        assert dm.error_code() == 0
+    finally:
+        dc.close()
+        c.close()
+        for e in ce + me:
+            e.close()
