@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import irisb200
+from irisb200.policy import prepare_or_policy_bitmap
 import workload as W
 
 pytestmark = pytest.mark.gpu
@@ -40,10 +41,8 @@ def test_two_eyes_or_policy(dm, oracle):
     right = _eye(dm, oracle, 0x5167, 22, {0: (5, 0), 1: (200, 0), 2: (300, 3), 4: (650, 1)})
     c = irisb200.Circuits(dm, W.SEEDS)
     dcs = [irisb200.DistanceComparator(dm, NQ, N_DB) for _ in range(2)]
-    policy_words = (N_DB + 63) // 64 * 2  # u32 words per query row of the internal bitmap
-    policy = np.zeros((NQ, policy_words), np.uint32)
-    for q, e in ((1, 100), (3, 650), (2, 300)):
-        policy[q, e // 32] |= np.uint32(1 << (e % 32))
+    # OR rule for (1, 100), (3, 650), (2, 300) (prepare_or_policy_bitmap)
+    policy = prepare_or_policy_bitmap(N_DB, [[], [100], [300], [650]], NQ)
     dpol = irisb200.DeviceBuffer.from_array(dm, policy)
     try:
         for (ce, me, _), dc in zip((left, right), dcs):
