@@ -1,0 +1,59 @@
+"""Parity at the benchmark's full size: 64 queries x 31 rotations against
+524,288 share-DB entries per party (3 parties, 60 GB resident).  The whole DB
+is scanned in one chunk and again in four chunks; the bitmaps must be equal
+(chunking invariance), every planted near-duplicate must be found, and blocks
+of entries at the start, the end and around the planted entries must equal
+the CPU path on the same shares (records read back from the device)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import irisb200
+import workload as W
+
+pytestmark = pytest.mark.gpu
+
+M, NQ, A = 524288, 64, 16384
+DB_SEED, Q_SEED = 0xDEADBEEF, 42
+
+
+def test_full_size_parity(dm, oracle):
+    planted = {j: (int((j * 7919 + 13) % M), (j * 7) % 31 - 15) for j in range(0, NQ, 10)}
+    ce = [irisb200.ShareDB(p, dm, M, NQ * 32, 12800, W.SEEDS[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, M, NQ * 32, 6400, W.SEEDS[p]) for p in range(3)]
+    c = irisb200.Circuits(dm, W.SEEDS)
+    dcs = [irisb200.DistanceComparator(dm, NQ, M) for _ in range(2)]
+    try:
+        for e in ce + me:
+            e.alloc_db(M)
+        irisb200.synth_db(ce, me, DB_SEED, 0, M)
+        qc, qm = irisb200.synth_queries(DB_SEED, Q_SEED, NQ, planted)
+        slots = [(j, 0, 31, j) for j in range(NQ)]
+        for p in range(3):
+            ce[p].query_upload_slots(qc[p], slots)
+            me[p].query_upload_slots(qm[p], slots)
+        mults = [1, 1, 1, 2, 2, 2]
+        irisb200.dot_many(ce + me, mults, 0, M)
+        dcs[0].compare_threshold_open(c, ce, me, 0, M, NQ, A)
+        for off in range(0, M, M // 4):
+            irisb200.dot_many(ce + me, mults, off, M // 4)
+            dcs[1].compare_threshold_open(c, ce, me, off, M // 4, NQ, A)
+        dm.synchronize()
+        bm = [irisb200.bitmap_get(dc.fetch_bitmap(NQ, M), NQ, M) for dc in dcs]
+        assert np.array_equal(bm[0], bm[1]), "one chunk and four chunks differ"
+        got = bm[0]
+        for j, (e, _) in planted.items():
+            assert got[j, e], f"planted query {j} -> {e} not found"
+        blocks = [(0, 1024), (M - 1024, 1024)] + [(max(0, min(e - 8, M - 16)), 16) for e, _ in planted.values()]
+        for first, n in blocks:
+            cs = np.stack([ce[p].fetch_records(first, n) for p in range(3)])
+            ms = np.stack([me[p].fetch_records(first, n) for p in range(3)])
+            exp = W.expected_bitmap(oracle, qc, qm, cs, ms, A)
+            assert np.array_equal(got[:, first:first + n], exp), f"entries {first}..{first + n}"
+    finally:
+        for dc in dcs:
+            dc.close()
+        c.close()
+        for e in ce + me:
+            e.close()
