@@ -1,9 +1,10 @@
 """Parity at the benchmark's full size: 64 queries x 31 rotations against
 524,288 share-DB entries per party (3 parties, 60 GB resident).  The whole DB
 is scanned in one chunk and again in four chunks; the bitmaps must be equal
-(chunking invariance), every planted near-duplicate must be found, and blocks
+(chunking invariance), every planted near-duplicate must be found, blocks
 of entries at the start, the end and around the planted entries must equal
-the CPU path on the same shares (records read back from the device)."""
+the CPU path on the same shares (records read back from the device), and the
+batched engine (packed rows, captured graph) must return the same matches."""
 from __future__ import annotations
 
 import numpy as np
@@ -51,6 +52,15 @@ def test_full_size_parity(dm, oracle):
             ms = np.stack([me[p].fetch_records(first, n) for p in range(3)])
             exp = W.expected_bitmap(oracle, qc, qm, cs, ms, A)
             assert np.array_equal(got[:, first:first + n], exp), f"entries {first}..{first + n}"
+        # the batched engine on the same queries (all 31 rotations) gives the same rows
+        from irisb200.batched import BatchedEngine, Request
+        eng = BatchedEngine(dm, ce, me, c, max_variants=NQ, max_reauth=16, threshold_a=A, autotune=False)
+        try:
+            res = eng.run([Request(code=qc[:, j], mask=qm[:, j]) for j in range(NQ)])
+        finally:
+            eng.close()
+        for j in range(NQ):
+            assert res[j].matches == np.nonzero(got[j])[0].tolist()[:256], f"batched query {j}"
     finally:
         for dc in dcs:
             dc.close()
