@@ -4,7 +4,9 @@ is scanned in one chunk and again in four chunks; the bitmaps must be equal
 (chunking invariance), every planted near-duplicate must be found, blocks
 of entries at the start, the end and around the planted entries must equal
 the CPU path on the same shares (records read back from the device), and the
-batched engine (packed rows, captured graph) must return the same matches."""
+batched engine (packed rows, captured graph) and the continuous server
+(chunked circular scan, requests admitted mid-scan) must return the same
+matches."""
 from __future__ import annotations
 
 import numpy as np
@@ -61,6 +63,17 @@ def test_full_size_parity(dm, oracle):
             eng.close()
         for j in range(NQ):
             assert res[j].matches == np.nonzero(got[j])[0].tolist()[:256], f"batched query {j}"
+        # and the continuous server (eight 65,536-entry steps per request, staggered arrivals)
+        from irisb200.serving import ContinuousServer
+        srv = ContinuousServer(dm, ce, me, c, chunk=65536, row_capacity=NQ * 32, max_variants=NQ, max_reauth=4,
+                               threshold_a=A, db_capacity=M)
+        try:
+            comps = srv.serve([0.002 * j for j in range(NQ)], [Request(code=qc[:, j], mask=qm[:, j])
+                                                               for j in range(NQ)])
+        finally:
+            srv.close()
+        for comp in comps:
+            assert comp.result.matches == np.nonzero(got[comp.idx])[0].tolist()[:256], f"served query {comp.idx}"
     finally:
         for dc in dcs:
             dc.close()
