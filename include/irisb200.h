@@ -159,6 +159,16 @@ int irs_device_fill_random(void* ptr, size_t bytes, uint64_t seed, void* stream)
  * block times the party's Lagrange coefficient at 0, converted to basis B. */
 int irs_preprocess_query_share(int party, uint16_t* coefs, size_t n);
 
+/* encode_iris_code / encode_mask_code (galois_engine.rs:319-397) of one iris
+ * (host): code_bits / mask_bits are the 12800 plaintext bits as u64 words
+ * [200] (bit i of the iris = bit i % 64 of word i / 64), seed drives the
+ * sharing randomness.  Writes the three parties' shares, code_out [3][12800]
+ * and the trimmed mask_out [3][6400]: DB records when preprocess = 0, query
+ * shares (irs_preprocess_query_share applied) otherwise.  A deletion writes
+ * the encoding of the default iris (all-zero code, full mask; the reference's
+ * get_dummy_shares_for_deletion, iris_db/mod.rs:10-23) over the record. */
+int irs_encode_iris(const uint64_t* code_bits, const uint64_t* mask_bits, uint64_t seed, int preprocess,
+                    uint16_t* code_out, uint16_t* mask_out);
 /* Seeded synthetic queries of the benchmark workload (host): query j is a
  * near-duplicate of DB entry planted_entry[j] (code bits flipped with p = 0.2,
  * rotated by planted_rot[j] columns) or, for planted_entry[j] < 0, a fresh

@@ -221,6 +221,20 @@ int irs_mirror_query_share(uint16_t* coefs, size_t n, int flip_imaginary) {
   return IRS_OK;
 }
 
+int irs_encode_iris(const uint64_t* code_bits, const uint64_t* mask_bits, uint64_t seed, int preprocess,
+                    uint16_t* code_out, uint16_t* mask_out) {
+  if (!code_bits || !mask_bits || !code_out || !mask_out) return IRS_ERR_INVALID;
+  u16* co[3];
+  u16* mo[3];
+  for (int p = 0; p < 3; p++) {
+    co[p] = code_out + (size_t)p * 12800;
+    mo[p] = mask_out + (size_t)p * 6400;
+  }
+  encode(code_bits, mask_bits, 0, seed, preprocess != 0, co, 12800);
+  encode(code_bits, mask_bits, 1, seed, preprocess != 0, mo, 6400);
+  return IRS_OK;
+}
+
 int irs_synth_queries(uint64_t db_seed, uint64_t q_seed, size_t n_queries, const int64_t* planted_entry,
                       const int32_t* planted_rot, int preprocess, uint16_t* code_out, uint16_t* mask_out) {
   if (!code_out || !mask_out) return IRS_ERR_INVALID;

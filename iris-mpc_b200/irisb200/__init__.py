@@ -76,6 +76,7 @@ _SIGS = {
     "irs_host_free_pinned": [_vp],
     "irs_preprocess_query_share": [_i, _vp, _sz],
     "irs_synth_queries": [_u64, _u64, _sz, _vp, _vp, _i, _vp, _vp],
+    "irs_encode_iris": [_vp, _vp, _u64, _i, _vp, _vp],
     "irs_copy_h2d": [_vp, _vp, _sz, _vp],
     "irs_copy_d2h": [_vp, _vp, _sz, _vp],
     "irs_stream_synchronize": [_vp],
@@ -278,6 +279,35 @@ class Graph:
         if self.h:
             lib().irs_graph_destroy(self.h)
             self.h = None
+
+
+def encode_iris(code_bits: np.ndarray, mask_bits: np.ndarray, seed: int, preprocess: bool = False):
+    """The three parties' shares of one iris (irs_encode_iris): code_bits /
+    mask_bits are u64 [200] (12800 bits).  Returns (code [3][12800], mask
+    [3][6400]) u16: DB records, or query shares when preprocess."""
+    c = np.ascontiguousarray(code_bits, np.uint64).reshape(200)
+    m = np.ascontiguousarray(mask_bits, np.uint64).reshape(200)
+    code = np.zeros((3, IRIS_CODE_LENGTH), np.uint16)
+    mask = np.zeros((3, MASK_CODE_LENGTH), np.uint16)
+    _check(lib().irs_encode_iris(_ptr(c), _ptr(m), seed, int(preprocess), _ptr(code), _ptr(mask)))
+    return code, mask
+
+
+def deletion_record(seed: int = 0):
+    """Shares of the default iris (all-zero code, full mask) that a deletion
+    writes over a DB record (get_dummy_shares_for_deletion,
+    iris-mpc-common/src/iris_db/mod.rs:10-23): it matches no real query."""
+    return encode_iris(np.zeros(200, np.uint64), np.full(200, 0xFFFFFFFFFFFFFFFF, np.uint64), seed)
+
+
+def delete_records(code_engines, mask_engines, indices, seed: int = 0) -> None:
+    """Deletions (actor.rs:2641-2680): the deletion record over each index of
+    the six engines (party p code at code_engines[p], mask at mask_engines[p])."""
+    code, mask = deletion_record(seed)
+    for idx in indices:
+        for p in range(3):
+            code_engines[p].load_records(int(idx), code[p][None])
+            mask_engines[p].load_records(int(idx), mask[p][None])
 
 
 def synth_queries(db_seed: int, q_seed: int, n_queries: int, planted: dict, preprocess: bool = True,
