@@ -76,6 +76,10 @@ int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_
  * without a host round trip: a serving loop that launches one DB chunk per
  * step draws fresh randomness for every step while the host runs ahead. */
 int irs_device_manager_advance_batch_counter(irs_device_manager* dm, void* stream);
+/* Reads the device batch counter (after the work queued on party 0's stream):
+ * with the parties' seeds and the DB length it is the whole randomness state
+ * to checkpoint (ChaChaCtx is (seed, counter), rng/chacha.rs:205-250). */
+int irs_device_manager_get_batch_counter(irs_device_manager* dm, uint64_t* batch_id);
 /* Number of SMs the persistent kernels size their grids to. */
 int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
 /* Host synchronisation of the calls that take host buffers (default on; no

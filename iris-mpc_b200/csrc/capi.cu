@@ -308,6 +308,15 @@ int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_
 
 __global__ void advance_batch_counter_kernel(uint64_t* b) { *b = *b % ((1ull << 24) - 1) + 1; }
 
+int irs_device_manager_get_batch_counter(irs_device_manager* dm, uint64_t* batch_id) {
+  CHECK(dm && batch_id, IRS_ERR_INVALID, "bad arguments");
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = dm->streams[0];
+  CU(cudaMemcpyAsync(batch_id, dm->d_batch, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return IRS_OK;
+}
+
 int irs_device_manager_advance_batch_counter(irs_device_manager* dm, void* stream) {
   CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
   CU(cudaSetDevice(dm->device));

@@ -97,6 +97,7 @@ _SIGS = {
     "irs_circuits_use_batch_counter": [_vp, _i],
     "irs_device_manager_set_batch_counter": [_vp, _u64, _vp],
     "irs_device_manager_advance_batch_counter": [_vp, _vp],
+    "irs_device_manager_get_batch_counter": [_vp, C.POINTER(_u64)],
     "irs_sharedb_query_upload_rows": [_vp, _vp, _sz, _vp, _sz],
     "irs_sharedb_gather_records": [_vp, _vp, _vp, _sz],
     "irs_sharedb_fill_random": [_vp, _u64, _sz],
@@ -378,6 +379,11 @@ class DeviceManager:
 
     def set_batch_counter(self, batch_id: int, stream=None) -> None:
         _check(lib().irs_device_manager_set_batch_counter(self.h, batch_id, stream))
+
+    def batch_counter(self) -> int:
+        v = _u64()
+        _check(lib().irs_device_manager_get_batch_counter(self.h, C.byref(v)))
+        return v.value
 
     def advance_batch_counter(self, stream=None) -> None:
         _check(lib().irs_device_manager_advance_batch_counter(self.h, stream))

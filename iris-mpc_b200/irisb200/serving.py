@@ -523,6 +523,24 @@ class ContinuousServer:
             self.dm.set_host_sync(True)
         return completions
 
+    def checkpoint(self) -> dict:
+        """The server's resumable state between serve() calls: the device
+        batch counter (with the parties' seeds, the whole ChaCha state) and
+        the DB length (the DB itself stays resident)."""
+        return {"batch_counter": self.dm.batch_counter(), "db_len": self.db_len}
+
+    def restore(self, state: dict) -> None:
+        """Resumes from checkpoint(): later steps draw fresh randomness after
+        the saved counter, and requests scan the saved DB length."""
+        if self.flight:
+            raise RuntimeError("restore() with requests in flight")
+        if state["db_len"] > self.db_capacity:
+            raise ValueError("checkpointed DB length exceeds the capacity")
+        self.dm.set_batch_counter(int(state["batch_counter"]))
+        self.db_len = int(state["db_len"])
+        for e in self.ce + self.me:
+            e.set_db_len(self.db_len)
+
     def close(self) -> None:
         for o in self.sce + self.sme + [self.dc, self.sdc]:
             o.close()

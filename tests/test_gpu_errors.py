@@ -111,3 +111,19 @@ def test_empty_inputs_are_no_ops(dm):
         c.close()
         for e in ce + me:
             e.close()
+
+
+def test_party_seed_ring_and_batch_counter(dm):
+    """Cross-party consistency: the circuits refuse seeds that do not form the
+    3-party ring (party p's second seed = party p-1's own seed); the device
+    batch counter reads back for checkpoints and advances on the stream."""
+    bad = [([0] * 8, [2] * 8), ([1] * 8, [9] * 8), ([2] * 8, [1] * 8)]
+    _raises(lambda: irisb200.Circuits(dm, bad), -1, "seed1 of party 1")
+    dm.set_batch_counter(123)
+    assert dm.batch_counter() == 123
+    dm.advance_batch_counter()
+    dm.advance_batch_counter()
+    assert dm.batch_counter() == 125
+    dm.set_batch_counter((1 << 24) - 1)
+    dm.advance_batch_counter()
+    assert dm.batch_counter() == 1  # wraps past 2^24 - 1 to 1 (0 is never used)

@@ -119,3 +119,8 @@ def test_serving_alone_equals_mix_and_cpu(oracle, world):
             assert res[i].reauth_mirror_match == bool(expm)
     assert res[2].reauth_match is True and res[8].reauth_match is True
     assert srv.steps > 0 and not srv.flight and len(srv.free_variants) == 32
+    # checkpoint / restore between serve() calls: the ChaCha batch counter and the DB length
+    state = srv.checkpoint()
+    assert state["db_len"] == N_DB + 1 and state["batch_counter"] >= srv.steps
+    srv.restore(state)
+    assert srv.dm.batch_counter() == state["batch_counter"] and srv.db_len == N_DB + 1
