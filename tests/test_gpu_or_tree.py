@@ -25,7 +25,7 @@ def _shares(rng, v):
 
 
 @pytest.mark.parametrize("n,planted", [(64 * 1000, []), (64 * 1000, [12345]), (64 * 3, [191]),
-                                       (64 * 777, [0, 40000])])
+                                       (64 * 777, [0, 40000]), (1 << 22, [(1 << 22) - 1])])
 def test_or_tree_matches_plaintext_and_oracle(dm, oracle, n, planted):
     rng = np.random.default_rng(n + len(planted))
     code = np.full(n, 65536 - 100, np.uint16)  # -100: no match against mask 1000
