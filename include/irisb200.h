@@ -76,6 +76,14 @@ int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_
  * without a host round trip: a serving loop that launches one DB chunk per
  * step draws fresh randomness for every step while the host runs ahead. */
 int irs_device_manager_advance_batch_counter(irs_device_manager* dm, void* stream);
+/* Stage timers (the reference's record_stream_time! / log_timers behind
+ * enable_debug_timing, server/actor.rs:71-85,2887-2911): while on, every dot
+ * launch ("dot") and threshold/open launch ("threshold_open") outside a graph
+ * capture is bracketed by CUDA events on its stream.  irs_device_manager_timings
+ * waits for them and writes "label=ms/launches;..." (summed since the last
+ * reset) into buf; reset != 0 clears the sums. */
+int irs_device_manager_set_timing(irs_device_manager* dm, int on);
+int irs_device_manager_timings(irs_device_manager* dm, char* buf, size_t cap, int reset);
 /* Reads the device batch counter (after the work queued on party 0's stream):
  * with the parties' seeds and the DB length it is the whole randomness state
  * to checkpoint (ChaChaCtx is (seed, counter), rng/chacha.rs:205-250). */

@@ -13,6 +13,8 @@
 
 #include <algorithm>
 #include <new>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "../../include/irisb200.h"
@@ -64,6 +66,37 @@ struct irs_device_manager {
   bool capturing = false;  // a graph capture on streams[0] is open
   cudaEvent_t graph_done = nullptr;  // recorded after each graph launch
   bool host_sync = true;  // false: host-buffer calls return once enqueued (irs_device_manager_set_host_sync)
+  // stage timers (irs_device_manager_set_timing): event pairs per label, resolved on read
+  bool timing = false;
+  struct Timer {
+    const char* label;
+    cudaEvent_t start, stop;
+  };
+  std::vector<Timer> timers;
+  std::map<std::string, std::pair<double, long>> timer_totals;  // label -> (ms, launches)
+};
+
+// Brackets one stage launch on stream s with a pair of timing events when the
+// device manager's stage timers are on (outside graph capture).
+struct StageTimer {
+  irs_device_manager* dm;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr, b = nullptr;
+  const char* label;
+  StageTimer(irs_device_manager* d, cudaStream_t st, const char* l) : dm(d), s(st), label(l) {
+    if (!dm->timing || dm->capturing) return;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+      cudaGetLastError();
+      a = b = nullptr;
+      return;
+    }
+    cudaEventRecord(a, s);
+  }
+  ~StageTimer() {
+    if (!a) return;
+    cudaEventRecord(b, s);
+    dm->timers.push_back({label, a, b});
+  }
 };
 
 struct irs_graph {
@@ -262,6 +295,10 @@ int irs_device_manager_destroy(irs_device_manager* dm) {
   cudaFree(dm->d_err);
   cudaFree(dm->d_batch);
   if (dm->graph_done) cudaEventDestroy(dm->graph_done);
+  for (auto& t : dm->timers) {
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
   for (int p = 0; p < 3; p++) {
     if (dm->streams[p]) cudaStreamDestroy(dm->streams[p]);
     if (dm->pools[p]) cudaMemPoolDestroy(dm->pools[p]);
@@ -307,6 +344,39 @@ int irs_device_manager_set_batch_counter(irs_device_manager* dm, uint64_t batch_
 }
 
 __global__ void advance_batch_counter_kernel(uint64_t* b) { *b = *b % ((1ull << 24) - 1) + 1; }
+
+int irs_device_manager_set_timing(irs_device_manager* dm, int on) {
+  CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
+  dm->timing = on != 0;
+  return IRS_OK;
+}
+
+int irs_device_manager_timings(irs_device_manager* dm, char* buf, size_t cap, int reset) {
+  CHECK(dm && buf && cap > 0, IRS_ERR_INVALID, "bad arguments");
+  CU(cudaSetDevice(dm->device));
+  for (auto& t : dm->timers) {
+    float ms = 0.f;
+    CU(cudaEventSynchronize(t.stop));
+    CU(cudaEventElapsedTime(&ms, t.start, t.stop));
+    auto& tot = dm->timer_totals[t.label];
+    tot.first += ms;
+    tot.second += 1;
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  dm->timers.clear();
+  std::string out;
+  char line[160];
+  for (auto& kv : dm->timer_totals) {
+    snprintf(line, sizeof line, "%s%s=%.6f/%ld", out.empty() ? "" : ";", kv.first.c_str(), kv.second.first,
+             kv.second.second);
+    out += line;
+  }
+  CHECK(out.size() + 1 <= cap, IRS_ERR_OVERFLOW, "timings need %zu bytes", out.size() + 1);
+  memcpy(buf, out.c_str(), out.size() + 1);
+  if (reset) dm->timer_totals.clear();
+  return IRS_OK;
+}
 
 int irs_device_manager_get_batch_counter(irs_device_manager* dm, uint64_t* batch_id) {
   CHECK(dm && batch_id, IRS_ERR_INVALID, "bad arguments");
@@ -867,7 +937,10 @@ int irs_sharedb_dot_many(irs_sharedb* const* engines, const uint16_t* multiplier
       CU(cudaEventRecord(engines[i]->done, dm->streams[engines[i]->peer]));
       CU(cudaStreamWaitEvent(s, engines[i]->done, 0));
     }
-  if (len) CU(launch_limb_gemm(P, engines[0]->block_n, dm->n_sms, s));
+  if (len) {
+    StageTimer timer(dm, s, "dot");
+    CU(launch_limb_gemm(P, engines[0]->block_n, dm->n_sms, s));
+  }
   for (int i = 0; i < n; i++) {
     engines[i]->res_offset = offset;
     engines[i]->res_len = len;
@@ -1270,7 +1343,10 @@ int irs_dc_compare_threshold_open(irs_distance_comparator* dc, irs_circuits* c, 
   P.match_list = self_check ? nullptr : dc->match_list;
   P.match_cap = (uint32_t)dc->match_cap;
   if (!self_check) set_distance_capture(dc, P);
-  CU(launch_threshold_bitmap(P, s));
+  {
+    StageTimer timer(dm, s, "threshold_open");
+    CU(launch_threshold_bitmap(P, s));
+  }
   if (slot_valid || slot_query) CU(cudaStreamSynchronize(s));  // host arrays are caller-owned
   return IRS_OK;
 }
@@ -1347,7 +1423,10 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
   P.match_list = self_check ? nullptr : dc->match_list;
   P.match_cap = (uint32_t)dc->match_cap;
   if (!self_check) set_distance_capture(dc, P);
-  CU(launch_threshold_bitmap(P, s));
+  {
+    StageTimer timer(dm, s, "threshold_open");
+    CU(launch_threshold_bitmap(P, s));
+  }
   return IRS_OK;
 }
 

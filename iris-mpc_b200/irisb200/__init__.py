@@ -98,6 +98,8 @@ _SIGS = {
     "irs_device_manager_set_batch_counter": [_vp, _u64, _vp],
     "irs_device_manager_advance_batch_counter": [_vp, _vp],
     "irs_device_manager_get_batch_counter": [_vp, C.POINTER(_u64)],
+    "irs_device_manager_set_timing": [_vp, _i],
+    "irs_device_manager_timings": [_vp, _vp, _sz, _i],
     "irs_sharedb_query_upload_rows": [_vp, _vp, _sz, _vp, _sz],
     "irs_sharedb_gather_records": [_vp, _vp, _vp, _sz],
     "irs_sharedb_fill_random": [_vp, _u64, _sz],
@@ -379,6 +381,21 @@ class DeviceManager:
 
     def set_batch_counter(self, batch_id: int, stream=None) -> None:
         _check(lib().irs_device_manager_set_batch_counter(self.h, batch_id, stream))
+
+    def set_timing(self, on: bool) -> None:
+        """Stage timers on the dot and threshold launches (debug timing)."""
+        _check(lib().irs_device_manager_set_timing(self.h, int(on)))
+
+    def timings(self, reset: bool = True) -> dict:
+        """{label: (total ms, launches)} of the stage timers."""
+        buf = C.create_string_buffer(4096)
+        _check(lib().irs_device_manager_timings(self.h, buf, len(buf), int(reset)))
+        out = {}
+        for item in filter(None, buf.value.decode().split(";")):
+            name, v = item.split("=")
+            ms, n = v.split("/")
+            out[name] = (float(ms), int(n))
+        return out
 
     def batch_counter(self) -> int:
         v = _u64()

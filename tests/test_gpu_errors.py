@@ -127,3 +127,38 @@ def test_party_seed_ring_and_batch_counter(dm):
     dm.set_batch_counter((1 << 24) - 1)
     dm.advance_batch_counter()
     assert dm.batch_counter() == 1  # wraps past 2^24 - 1 to 1 (0 is never used)
+
+
+def test_stage_timers(dm):
+    """Debug stage timers: with timing on, each dot and threshold launch is
+    timed on its stream; the sums read back per label and reset."""
+    ce = [irisb200.ShareDB(p, dm, 256, 64, 12800, W.SEEDS[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, 256, 64, 6400, W.SEEDS[p]) for p in range(3)]
+    c = irisb200.Circuits(dm, W.SEEDS)
+    dc = irisb200.DistanceComparator(dm, 2, 256)
+    try:
+        slots = [(0, 0, 31, 0), (0, 0, 31, 1)]
+        for p in range(3):
+            ce[p].alloc_db(256)
+            me[p].alloc_db(256)
+            ce[p].fill_random(p, 256)
+            me[p].fill_random(10 + p, 256)
+            ce[p].query_upload_slots(np.ones((1, 12800), np.uint16), slots)
+            me[p].query_upload_slots(np.ones((1, 6400), np.uint16), slots)
+        dm.timings(reset=True)
+        dm.set_timing(True)
+        for _ in range(3):
+            irisb200.dot_many(ce + me, [1, 1, 1, 2, 2, 2], 0, 256)
+            dc.compare_threshold_open(c, ce, me, 0, 256, 2, 16384)
+        t = dm.timings(reset=True)
+        assert t["dot"][1] == 3 and t["threshold_open"][1] == 3
+        assert t["dot"][0] > 0 and t["threshold_open"][0] > 0
+        dm.set_timing(False)
+        irisb200.dot_many(ce + me, [1, 1, 1, 2, 2, 2], 0, 256)
+        assert dm.timings() == {}
+    finally:
+        dm.set_timing(False)
+        dc.close()
+        c.close()
+        for e in ce + me:
+            e.close()
