@@ -171,6 +171,19 @@ def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
 
+def _host_arg(dm, a, dtype) -> np.ndarray:
+    """A host buffer for a call that may only enqueue its copy: with the
+    device manager's host synchronisation off the library reads the buffer
+    after the call returns, so a converted temporary copy would be freed too
+    early -- such calls take the caller's own C-contiguous array or fail."""
+    if getattr(dm, "host_sync", True):
+        return np.ascontiguousarray(a, dtype)
+    if not isinstance(a, np.ndarray) or a.dtype != np.dtype(dtype) or not a.flags.c_contiguous:
+        raise ValueError("with host synchronisation off, pass a C-contiguous %s array that stays alive and "
+                         "unchanged until the work has run (page-locked memory: PinnedArray)" % np.dtype(dtype))
+    return a
+
+
 def _seed(s) -> np.ndarray:
     return np.ascontiguousarray(np.array(s, dtype=np.uint32).reshape(8))
 
@@ -365,6 +378,7 @@ class DeviceManager:
         _check(lib().irs_device_manager_init(device, C.byref(h)))
         self.h = h.value
         self.device = device
+        self.host_sync = True
 
     def stream(self, party: int):
         s = _vp()
@@ -408,6 +422,7 @@ class DeviceManager:
     def set_host_sync(self, on: bool) -> None:
         """See irs_device_manager_set_host_sync: off = enqueue-only calls on pinned host buffers."""
         _check(lib().irs_device_manager_set_host_sync(self.h, int(on)))
+        self.host_sync = bool(on)
 
     def mem_info(self):
         f, t = _sz(), _sz()
@@ -485,18 +500,18 @@ class ShareDB:
 
     def query_upload_rows(self, base: np.ndarray, row_desc) -> None:
         """Rows row_desc[r] = (src << 8) | rotation, 0xFFFFFFFF = empty."""
-        b = np.ascontiguousarray(base, np.uint16).reshape(-1, self.code_length)
-        rd = np.ascontiguousarray(row_desc, np.uint32)
+        b = _host_arg(self.dm, base, np.uint16).reshape(-1, self.code_length)
+        rd = _host_arg(self.dm, row_desc, np.uint32)
         _check(lib().irs_sharedb_query_upload_rows(self.h, _ptr(b), b.shape[0], _ptr(rd), rd.size))
 
     def query_put_base(self, first: int, base: np.ndarray) -> None:
         """Writes base queries [first, first + len(base)) of the resident pool."""
-        b = np.ascontiguousarray(base, np.uint16).reshape(-1, self.code_length)
+        b = _host_arg(self.dm, base, np.uint16).reshape(-1, self.code_length)
         _check(lib().irs_sharedb_query_put_base(self.h, first, b.shape[0], _ptr(b)))
 
     def query_expand_rows(self, n_base: int, row_desc) -> None:
         """query_upload_rows over the resident pool [0, n_base)."""
-        rd = np.ascontiguousarray(row_desc, np.uint32)
+        rd = _host_arg(self.dm, row_desc, np.uint32)
         _check(lib().irs_sharedb_query_expand_rows(self.h, n_base, _ptr(rd), rd.size))
 
     def fill_random(self, seed: int, n: int) -> None:
@@ -505,7 +520,7 @@ class ShareDB:
 
     def gather_records(self, src: "ShareDB", ids) -> None:
         """prefetch_subset: records ids[k] of src become records k of this engine."""
-        i = np.ascontiguousarray(ids, np.uint32)
+        i = _host_arg(self.dm, ids, np.uint32)
         _check(lib().irs_sharedb_gather_records(self.h, src.h, _ptr(i), i.size))
 
     def dot(self, offset: int, length: int, multiplier: int = 1, stream=None) -> None:
@@ -622,9 +637,9 @@ class DistanceComparator:
             int(self_check), stream))
 
     def set_segments(self, seg_start, seg_query, seg_mask) -> None:
-        st = np.ascontiguousarray(seg_start, np.uint32)
-        sq = np.ascontiguousarray(seg_query, np.uint32)
-        sm = np.ascontiguousarray(seg_mask, np.uint32)
+        st = _host_arg(self.dm, seg_start, np.uint32)
+        sq = _host_arg(self.dm, seg_query, np.uint32)
+        sm = _host_arg(self.dm, seg_mask, np.uint32)
         _check(lib().irs_dc_set_segments(self.h, st.size - 1, _ptr(st), _ptr(sq) if sq.size else None,
                                          _ptr(sm) if sm.size else None))
 

@@ -186,3 +186,27 @@ def test_full_face_mirror_attack_rule():
     r = Request(code=None, mask=None, mirrored=True, kind="reauth", target=1)
     assert not full_face_mirror_attack(r, Result(matches=[], mirror_matches=[7]))
     assert not full_face_mirror_attack(Request(code=None, mask=None), Result(matches=[], mirror_matches=[7]))
+
+
+def test_async_host_mode_refuses_temporaries():
+    """With host synchronisation off the library reads host buffers after the
+    call returns: a list or a converted copy would be freed too early, so the
+    bindings refuse it; with it on they convert as usual."""
+    import pytest
+
+    from irisb200 import _host_arg
+
+    class _Dm:
+        host_sync = True
+
+    dm = _Dm()
+    a = np.arange(8, dtype=np.uint32)
+    assert _host_arg(dm, a, np.uint32) is a
+    assert _host_arg(dm, [1, 2, 3], np.uint32).dtype == np.uint32
+    assert _host_arg(dm, a.astype(np.int64), np.uint32).dtype == np.uint32
+    dm.host_sync = False
+    assert _host_arg(dm, a, np.uint32) is a
+    assert _host_arg(dm, a[2:6], np.uint32).base is a
+    for bad in ([1, 2, 3], a.astype(np.int64), a[::2]):
+        with pytest.raises(ValueError):
+            _host_arg(dm, bad, np.uint32)
