@@ -79,10 +79,42 @@ struct WordRand {
 // Gate g (compile-time after unrolling) must lie in the loaded block.
 #define IRS_GATE(wr, x, y, g) cand((x), (y), (wr).ks[0][(g) & 15], (wr).ks[1][(g) & 15], (wr).ks[2][(g) & 15])
 
+// Byte select from the pair (a, b): result byte i = byte ((sel >> 4i) & 7)
+// of the 8-byte value b:a (one PRMT on the device).
+IRS_HD uint32_t select_bytes(uint32_t a, uint32_t b, uint32_t sel) {
+#ifdef __CUDA_ARCH__
+  return __byte_perm(a, b, sel);
+#else
+  const uint64_t v = ((uint64_t)b << 32) | a;
+  uint32_t r = 0;
+  for (int i = 0; i < 4; i++) r |= (uint32_t)((v >> (8 * ((sel >> (4 * i)) & 7))) & 0xFFu) << (8 * i);
+  return r;
+#endif
+}
+
+// The first two butterfly stages of the transpose, which move whole half
+// words and bytes: (lo a | lo b << 16, hi a | hi b << 16) and the byte
+// interleave of the stage with mask 0x00FF00FF -- one byte select per output.
+IRS_HD void swap_halves(uint32_t& a, uint32_t& b) {
+  const uint32_t x = select_bytes(a, b, 0x5410), y = select_bytes(a, b, 0x7632);
+  a = x;
+  b = y;
+}
+IRS_HD void swap_bytes(uint32_t& a, uint32_t& b) {
+  const uint32_t x = select_bytes(a, b, 0x6240), y = select_bytes(a, b, 0x7351);
+  a = x;
+  b = y;
+}
+
 // In-register 32x32 bit transpose: afterwards A[r] bit c = old A[c] bit r.
 IRS_HD void transpose32(uint32_t A[32]) {
 #pragma unroll
-  for (int s = 16, m = 0x0000FFFF; s > 0; s >>= 1, m ^= (m << s)) {
+  for (int k = 0; k < 16; k++) swap_halves(A[k], A[k + 16]);
+#pragma unroll
+  for (int k = 0; k < 32; k++)
+    if ((k & 8) == 0) swap_bytes(A[k], A[k + 8]);
+#pragma unroll
+  for (int s = 4, m = 0x0F0F0F0F; s > 0; s >>= 1, m ^= (m << s)) {
 #pragma unroll
     for (int k = 0; k < 32; k++) {
       if ((k & s) == 0) {
@@ -107,7 +139,10 @@ IRS_HD void slice16(const uint32_t w[16], uint32_t P[16]) {
   }
   // 16x16 transposes of both halves at once (the s = 8..1 stages of transpose32)
 #pragma unroll
-  for (int s = 8, m = 0x00FF00FF; s > 0; s >>= 1, m ^= (m << s)) {
+  for (int k = 0; k < 16; k++)
+    if ((k & 8) == 0) swap_bytes(A[k], A[k + 8]);
+#pragma unroll
+  for (int s = 4, m = 0x0F0F0F0F; s > 0; s >>= 1, m ^= (m << s)) {
 #pragma unroll
     for (int k = 0; k < 16; k++) {
       if ((k & s) == 0) {

@@ -55,8 +55,10 @@ __global__ void __launch_bounds__(kThreshThreads) threshold_flat_kernel(const Th
   }
 }
 
-template <int MIN_BLOCKS>
-__global__ void __launch_bounds__(kThreshThreads, MIN_BLOCKS) threshold_bitmap_kernel(const ThresholdParams P) {
+// The bitmap kernel indexes by global warp only, so its block size is free:
+// THREADS x MIN_BLOCKS sets the resident warps per SM the registers are sized for.
+template <int THREADS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) threshold_bitmap_kernel(const ThresholdParams P) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t n_groups = (P.n_entries + 31) / 32;
@@ -72,10 +74,15 @@ __global__ void __launch_bounds__(kThreshThreads, MIN_BLOCKS) threshold_bitmap_k
   WordRand wr;
   init_rand(wr, P, ((uint64_t)P.m0 + m_read) * (uint64_t)(P.n_pad / 32) + slot);
   const size_t off = (size_t)m_read * P.n_pad + (size_t)slot * 32;
-  const uint16_t* code[3] = {P.code[0] + off, P.code[1] + off, P.code[2] + off};
-  const uint16_t* mask[3] = {P.mask[0] + off, P.mask[1] + off, P.mask[2] + off};
-  Comp msb;
-  const uint32_t opened = threshold_word<kStageFull>(code, mask, P.threshold_a, wr, msb);
+  uint32_t opened;
+  {
+    // The share pointers die here; the rare distance capture below rebuilds
+    // them from `off`, which keeps 12 registers free through the circuit.
+    const uint16_t* code[3] = {P.code[0] + off, P.code[1] + off, P.code[2] + off};
+    const uint16_t* mask[3] = {P.mask[0] + off, P.mask[1] + off, P.mask[2] + off};
+    Comp msb;
+    opened = threshold_word<kStageFull>(code, mask, P.threshold_a, wr, msb);
+  }
   const size_t bitmap_word = (size_t)((P.m0 + group * 32) / 32);
   // Rotation OR of one query's rows, one ballot for the warp's 32 entries.
   auto emit = [&](uint32_t query, uint32_t row_mask, bool shared_word) {
@@ -137,8 +144,8 @@ __global__ void __launch_bounds__(kThreshThreads, MIN_BLOCKS) threshold_bitmap_k
         P.dist_row[pos] = slot * 32 + (uint32_t)r;
 #pragma unroll
         for (int p = 0; p < 3; p++) {
-          P.dist_code[(size_t)p * P.dist_cap + pos] = code[p][r];
-          P.dist_mask[(size_t)p * P.dist_cap + pos] = mask[p][r];
+          P.dist_code[(size_t)p * P.dist_cap + pos] = P.code[p][off + r];
+          P.dist_mask[(size_t)p * P.dist_cap + pos] = P.mask[p][off + r];
         }
       }
     }
@@ -176,18 +183,19 @@ cudaError_t launch_threshold_flat(const ThresholdParams& P, int stage, cudaStrea
 cudaError_t launch_threshold_bitmap(const ThresholdParams& P, cudaStream_t stream) {
   if (P.n_entries == 0 || P.n_slots == 0) return cudaSuccess;
   const uint64_t warps = (uint64_t)((P.n_entries + 31) / 32) * P.n_slots;
-  const uint64_t threads = warps * 32;
-  const unsigned grid = (unsigned)((threads + kThreshThreads - 1) / kThreshThreads);
-  // Occupancy variant (blocks of 128 threads per SM the registers are sized
-  // for); IRS_THRESHOLD_MIN_BLOCKS overrides the default for tuning runs.
-  static int min_blocks = [] {
-    const char* e = getenv("IRS_THRESHOLD_MIN_BLOCKS");
-    const int v = e ? atoi(e) : 2;
-    return (v == 3 || v == 4) ? v : 2;
+  // Resident warps per SM the kernel's registers are sized for: 12 (3 per
+  // SM sub-partition: 168 registers with a 48-byte spill) measured 4-6%
+  // faster than 8 (195 registers, no spill) on 512K-entry batches.  Other
+  // counts give the same register cap as one of these two, since each
+  // sub-partition holds a quarter of the register file.
+  // IRS_THRESHOLD_WARPS_PER_SM=8 selects the other variant for tuning runs.
+  static const bool eight = [] {
+    const char* e = getenv("IRS_THRESHOLD_WARPS_PER_SM");
+    return e && atoi(e) == 8;
   }();
-  if (min_blocks == 4) threshold_bitmap_kernel<4><<<grid, kThreshThreads, 0, stream>>>(P);
-  else if (min_blocks == 3) threshold_bitmap_kernel<3><<<grid, kThreshThreads, 0, stream>>>(P);
-  else threshold_bitmap_kernel<2><<<grid, kThreshThreads, 0, stream>>>(P);
+  const unsigned grid = (unsigned)((warps * 32 + kThreshThreads - 1) / kThreshThreads);
+  if (eight) threshold_bitmap_kernel<kThreshThreads, 2><<<grid, kThreshThreads, 0, stream>>>(P);
+  else threshold_bitmap_kernel<kThreshThreads, 3><<<grid, kThreshThreads, 0, stream>>>(P);
   return cudaGetLastError();
 }
 
