@@ -210,11 +210,14 @@ typedef struct irs_query_slot {
 int irs_sharedb_query_upload_slots(irs_sharedb* db, const uint16_t* base, size_t n_base,
                                    const irs_query_slot* slots, size_t n_slots);
 /* Uploads preprocessed base queries [n_base][code_length] and fills query row
- * r with row_desc[r] = (src << 8) | rotation (rotation 0..30 of base query src,
- * 15 = centre), 0xFFFFFFFF = zero row.  Packs queries with any rotation count
- * densely (the batched launch of uneven requests).  No counterpart in the
- * reference, which gives every query a block of 31 rotation rows
- * (htod_transfer_query, device_manager.rs:159-212). */
+ * r with row_desc[r] = (src << 8) | (mirror << 7) | rotation (rotation 0..30
+ * of base query src, 15 = centre; mirror = 1: of its mirrored form, the
+ * reference's mirrored_code / mirrored_mask, galois_engine.rs:218-225,520-543,
+ * applied on the device), 0xFFFFFFFF = zero row.  Packs queries with any
+ * rotation count densely (the batched launch of uneven requests); a request
+ * and its mirror share one base.  No counterpart in the reference, which
+ * gives every query a block of 31 rotation rows (htod_transfer_query,
+ * device_manager.rs:159-212) and mirrors on the host. */
 int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t n_base, const uint32_t* row_desc,
                                   size_t n_rows);
 /* Resident base-query pool for a serving loop (no counterpart in the

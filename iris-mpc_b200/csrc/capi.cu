@@ -787,7 +787,7 @@ int irs_sharedb_query_upload_rows(irs_sharedb* db, const uint16_t* base, size_t 
   const size_t base_bytes = n_base * K * 2, table_bytes = n_rows * 4;
   CHECK(base_bytes + table_bytes + 16 <= db->n_cap * K * 2, IRS_ERR_INVALID, "too many base queries for the staging");
   for (size_t r = 0; r < n_rows; r++)
-    CHECK(row_desc[r] == 0xFFFFFFFFu || ((row_desc[r] >> 8) < n_base && (row_desc[r] & 0xFFu) < (uint32_t)kRotations),
+    CHECK(row_desc[r] == 0xFFFFFFFFu || ((row_desc[r] >> 8) < n_base && (row_desc[r] & 0x7Fu) < (uint32_t)kRotations),
           IRS_ERR_INVALID, "row %zu descriptor 0x%x is invalid", r, row_desc[r]);
   int rc = set_active_rows(db, n_rows);
   if (rc) return rc;
@@ -828,7 +828,7 @@ int irs_sharedb_query_expand_rows(irs_sharedb* db, size_t n_base, const uint32_t
   const size_t base_bytes = n_base * K * 2, table_bytes = n_rows * 4;
   CHECK(base_bytes + table_bytes + 16 <= db->n_cap * K * 2, IRS_ERR_INVALID, "pool and row table exceed the staging");
   for (size_t r = 0; r < n_rows; r++)
-    CHECK(row_desc[r] == 0xFFFFFFFFu || ((row_desc[r] >> 8) < n_base && (row_desc[r] & 0xFFu) < (uint32_t)kRotations),
+    CHECK(row_desc[r] == 0xFFFFFFFFu || ((row_desc[r] >> 8) < n_base && (row_desc[r] & 0x7Fu) < (uint32_t)kRotations),
           IRS_ERR_INVALID, "row %zu descriptor 0x%x is invalid", r, row_desc[r]);
   int rc = set_active_rows(db, n_rows);
   if (rc) return rc;

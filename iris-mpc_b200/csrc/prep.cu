@@ -65,10 +65,18 @@ __global__ void expand_slots_kernel(const uint16_t* __restrict__ base, uint32_t 
   reinterpret_cast<uint32_t*>(hi)[i] = h;
 }
 
-// One thread per (row, 4-coefficient block).  row_desc[r] = (src << 8) | rot
-// puts rotation `rot` (0..30, 15 = centre) of base query `src` in row r;
+// One thread per (row, 4-coefficient block).  row_desc[r] = (src << 8) |
+// mirror << 7 | rot puts rotation `rot` (0..30, 15 = centre) of base query
+// `src` in row r, of its mirrored form when the mirror bit is set;
 // 0xFFFFFFFF leaves the row zero.  Lets a batch pack queries with different
 // rotation counts densely (no 32-row slot per query).
+//
+// Mirror (mirrored_code / mirrored_mask of the query share,
+// iris-mpc-common/src/galois_engine.rs:218-225,520-543): 4-coefficient
+// column c of each 800-coefficient row moves to 99 - c (c < 100) or 299 - c
+// (c >= 100), and a code share's imaginary half (rows 8..15) is negated.
+// The column map is its own inverse, so rotated row column `col` reads base
+// column mirror((col + left) mod 200).
 __global__ void expand_rows_kernel(const uint16_t* __restrict__ base, uint32_t K, const uint32_t* __restrict__ row_desc,
                                    uint32_t n_rows, uint32_t n_pad, uint8_t* __restrict__ lo, uint8_t* __restrict__ hi) {
   const uint32_t blocks_per_row = K / 4;
@@ -79,11 +87,17 @@ __global__ void expand_rows_kernel(const uint16_t* __restrict__ base, uint32_t K
   uint32_t l = 0, h = 0;
   const uint32_t d = row < n_rows ? row_desc[row] : 0xFFFFFFFFu;
   if (d != 0xFFFFFFFFu) {
-    const uint32_t src = d >> 8, rot = d & 0xFFu;
+    const uint32_t src = d >> 8, rot = d & 0x7Fu;
+    const bool mirror = (d & 0x80u) != 0;
     const int left_blocks = 15 - (int)rot;
     const uint32_t row800 = b / 200, col = b % 200;
-    const uint32_t src_col = (uint32_t)(((int)col + left_blocks % 200 + 200) % 200);
-    const uint2 v = *reinterpret_cast<const uint2*>(base + (size_t)src * K + (size_t)row800 * kRowLen + (size_t)src_col * 4);
+    uint32_t src_col = (uint32_t)(((int)col + left_blocks % 200 + 200) % 200);
+    if (mirror) src_col = src_col < 100 ? 99 - src_col : 299 - src_col;
+    uint2 v = *reinterpret_cast<const uint2*>(base + (size_t)src * K + (size_t)row800 * kRowLen + (size_t)src_col * 4);
+    if (mirror && row800 >= 8) {  // imaginary half: only code shares reach it
+      v.x = sub2(0u, v.x);
+      v.y = sub2(0u, v.y);
+    }
     l = (v.x & 0xFFu) | ((v.x >> 8) & 0xFF00u) | ((v.y & 0xFFu) << 16) | ((v.y & 0xFF0000u) << 8);
     h = ((v.x >> 8) & 0xFFu) | ((v.x >> 16) & 0xFF00u) | ((v.y & 0xFF00u) << 8) | (v.y & 0xFF000000u);
   }

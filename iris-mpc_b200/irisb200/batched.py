@@ -27,7 +27,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import (IRIS_CODE_LENGTH, MASK_CODE_LENGTH, MAX_MATCHES_LEN, Circuits, DeviceManager, DistanceComparator,
-               Graph, ShareDB, dot_many, mirror_query_share)
+               Graph, ShareDB, dot_many)
 
 MULTS = [1, 1, 1, 2, 2, 2]
 
@@ -72,7 +72,7 @@ def full_face_mirror_attack(request: Request, result: Result) -> bool:
 @dataclass
 class Layout:
     """Dense packing of the variants' rows into 32-row words."""
-    row_desc: np.ndarray   # [rows] (src << 8) | rotation, 0xFFFFFFFF = empty
+    row_desc: np.ndarray   # [rows] (src << 8) | (mirror << 7) | rotation, 0xFFFFFFFF = empty
     seg_start: np.ndarray  # [n_slots + 1]
     seg_query: np.ndarray  # [n_seg] variant index (bitmap row)
     seg_mask: np.ndarray   # [n_seg] rows of the slot belonging to the variant
@@ -110,6 +110,18 @@ def pack(variant_rows: list) -> Layout:
         seg_start.append(len(seg_query))
     return Layout(row_desc, np.array(seg_start, np.uint32), np.array(seg_query, np.uint32),
                   np.array(seg_mask, np.uint32), n_slots * 32, n_slots)
+
+
+def attach_bases(layout: Layout, base_of, mirrored) -> Layout:
+    """Points the rows of variant v at base query base_of[v], mirrored on the
+    device (bit 7 of the row descriptor) when mirrored[v]: a request and its
+    mirrored variant share one uploaded base."""
+    d = layout.row_desc.copy()
+    live = d != 0xFFFFFFFF
+    v = d[live] >> 8
+    flag = np.where(np.asarray(mirrored, bool)[v], 0x80, 0).astype(np.uint32)
+    d[live] = (np.asarray(base_of, np.uint32)[v] << 8) | flag | (d[live] & 0x7F)
+    return Layout(d, layout.seg_start, layout.seg_query, layout.seg_mask, layout.n_rows, layout.n_slots)
 
 
 def padded_rows(n_rows: int, cap: int) -> int:
@@ -244,20 +256,26 @@ class BatchedEngine:
         self.batch_id = (self.batch_id + 1) % (1 << 24) or 1
         return results
 
-    def _base(self, requests, variants):
-        code = np.zeros((3, len(variants), IRIS_CODE_LENGTH), np.uint16)
-        mask = np.zeros((3, len(variants), MASK_CODE_LENGTH), np.uint16)
-        for v, (i, mir) in enumerate(variants):
-            r = requests[i]
-            for p in range(3):
-                code[p, v] = mirror_query_share(r.code[p], True) if mir else r.code[p]
-                mask[p, v] = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
-        return code, mask
+    @staticmethod
+    def _bases(requests, variants):
+        """One base share per request (a mirrored variant reads its request's
+        base through the mirror bit): (code [3][n][12800], mask [3][n][6400],
+        base index per variant, mirrored flag per variant)."""
+        order = list(dict.fromkeys(i for i, _ in variants))
+        index = {i: k for k, i in enumerate(order)}
+        code = np.empty((3, len(order), IRIS_CODE_LENGTH), np.uint16)
+        mask = np.empty((3, len(order), MASK_CODE_LENGTH), np.uint16)
+        for k, i in enumerate(order):
+            code[:, k] = requests[i].code
+            mask[:, k] = requests[i].mask
+        return code, mask, [index[i] for i, _ in variants], [mir for _, mir in variants]
+
+    def _layout(self, requests, variants, base_of, mirrored) -> Layout:
+        return attach_bases(pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants]), base_of, mirrored)
 
     def _run_uniqueness(self, requests, variants, results):
-        layout = pad_rows(pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants]),
-                          self.ce[0].query_length)
-        code, mask = self._base(requests, variants)
+        code, mask, base_of, mirrored = self._bases(requests, variants)
+        layout = pad_rows(self._layout(requests, variants, base_of, mirrored), self.ce[0].query_length)
         for p in range(3):
             self.ce[p].query_upload_rows(code[p], layout.row_desc)
             self.me[p].query_upload_rows(mask[p], layout.row_desc)
@@ -277,8 +295,8 @@ class BatchedEngine:
         for p in range(3):
             self.sce[p].gather_records(self.ce[p], ids)
             self.sme[p].gather_records(self.me[p], ids)
-        layout = pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants])
-        code, mask = self._base(requests, variants)
+        code, mask, base_of, mirrored = self._bases(requests, variants)
+        layout = self._layout(requests, variants, base_of, mirrored)
         for p in range(3):
             self.sce[p].query_upload_rows(code[p], layout.row_desc)
             self.sme[p].query_upload_rows(mask[p], layout.row_desc)

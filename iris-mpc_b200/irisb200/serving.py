@@ -37,7 +37,7 @@ import numpy as np
 
 from . import (IRIS_CODE_LENGTH, MASK_CODE_LENGTH, MAX_MATCHES_LEN, DistanceComparator, Event, IrisError,
                PinnedArray, ShareDB, dot_many, mirror_query_share)
-from .batched import MULTS, Request, Result, centred_rotations, pack, padded_rows
+from .batched import MULTS, Request, Result, attach_bases, centred_rotations, pack, padded_rows
 
 RESULT_BYTES_PER_ROW_ENTRY = 2 * 6  # u16 dot share per (row, entry) for 6 engines
 
@@ -226,8 +226,9 @@ class ContinuousServer:
 
     def admit(self, r: Request, idx: int, arrival: float) -> None:
         """Places the request's variants and writes their base shares into
-        the host mirror of the pool (pool index = bitmap row); the next step
-        copies them to the device."""
+        the host copy of the pool (pool index = bitmap row); the next step
+        copies them to the device.  A mirrored variant's slot holds the plain
+        share: its rows carry the mirror bit and the device mirrors them."""
         variants = []
         for mir in ([False, True] if r.mirrored else [False]):
             where = self._place(r.n_rot)
@@ -237,8 +238,8 @@ class ContinuousServer:
             self._occupy(v, *where)
             variants.append(v)
             for p in range(3):
-                self.h_pool_c.array[p, v.vid] = mirror_query_share(r.code[p], True) if mir else r.code[p]
-                self.h_pool_m.array[p, v.vid] = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
+                self.h_pool_c.array[p, v.vid] = r.code[p]
+                self.h_pool_m.array[p, v.vid] = r.mask[p]
             self.pending_bases.add(v.vid)
         f = _Flight(r, idx, arrival, self.db_len, variants, set(range(math.ceil(self.db_len / self.chunk))))
         self.flight.append(f)
@@ -256,7 +257,8 @@ class ContinuousServer:
         for s in range(n_slots):
             for v in sorted(self.slot_vars[s], key=lambda x: x.first):
                 n = len(v.rots)
-                row_desc[s * 32 + v.first: s * 32 + v.first + n] = (v.vid << 8) | np.array(v.rots, np.uint32)
+                row_desc[s * 32 + v.first: s * 32 + v.first + n] = \
+                    (v.vid << 8) | (0x80 if v.mirrored else 0) | np.array(v.rots, np.uint32)
                 seg_query.append(v.vid)
                 seg_mask.append((((1 << n) - 1) << v.first) & 0xFFFFFFFF)
             seg_start.append(len(seg_query))
@@ -323,13 +325,14 @@ class ContinuousServer:
         for p in range(3):
             self.sce[p].gather_records(self.ce[p], ids)
             self.sme[p].gather_records(self.me[p], ids)
-        layout = pack([list(centred_rotations(items[j][2].n_rot)) for j, _ in variants])
+        layout = attach_bases(pack([list(centred_rotations(items[j][2].n_rot)) for j, _ in variants]),
+                              range(n), [mir for _, mir in variants])
         bc, bm = (x.array for x in self.h_r_base[par])
-        for v, (j, mir) in enumerate(variants):
+        for v, (j, _) in enumerate(variants):
             r = items[j][2]
             for p in range(3):
-                bc[p, v] = mirror_query_share(r.code[p], True) if mir else r.code[p]
-                bm[p, v] = mirror_query_share(r.mask[p], False) if mir else r.mask[p]
+                bc[p, v] = r.code[p]
+                bm[p, v] = r.mask[p]
         rt = self.h_r_rows[par].array[: layout.n_rows]
         rt[:] = layout.row_desc
         for p in range(3):
