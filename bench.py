@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: arrival window per load")
     ap.add_argument("--chunk", type=int, default=65536, help="serving: DB chunk per step")
     ap.add_argument("--serving-arms", default="served,plain", help="serving: which servers to run")
-    ap.add_argument("--serving-rate", type=float, default=500.0,
+    ap.add_argument("--serving-rate", type=float, default=600.0,
                     help="default run: offered load of its serving leg, requests/s (0 = skip)")
     return ap.parse_args()
 
