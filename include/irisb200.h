@@ -94,12 +94,14 @@ int irs_device_manager_sm_count(irs_device_manager* dm, int* n);
  * counterpart in the reference, whose calls are stream-ordered cudarc copies).
  * With it off, irs_sharedb_query_put_base, irs_sharedb_query_expand_rows,
  * irs_sharedb_query_upload_rows, irs_sharedb_gather_records,
- * irs_dc_set_segments and irs_dc_take_rows return as soon as their copies and
- * kernels are enqueued: their host buffers must then be page-locked
- * (irs_host_alloc_pinned) and stay unchanged until the work has run, and
- * take_rows outputs are valid after an event recorded behind them on the
- * party-0 stream has completed (device errors: irs_device_manager_error).  A
- * serving loop uses this to prepare and launch step k+1 while step k runs. */
+ * irs_dc_set_segments, irs_dc_take_rows, irs_dc_fetch_rows and
+ * irs_dc_fetch_final_results return as soon as their copies and kernels are
+ * enqueued: their host buffers must then be page-locked
+ * (irs_host_alloc_pinned) and stay unchanged until the work has run, and the
+ * outputs of the last three are valid after an event recorded behind them on
+ * the party-0 stream has completed (device
+ * errors: irs_device_manager_error).  A serving loop or a batched caller uses
+ * this to prepare and launch batch k+1 while batch k runs. */
 int irs_device_manager_set_host_sync(irs_device_manager* dm, int on);
 /* CUDA events for the asynchronous mode (cudaEventDisableTiming); the
  * reference uses raw CUevents through cudarc (device_manager.rs). */
@@ -427,7 +429,10 @@ int irs_dc_join_batch_matches(irs_distance_comparator* dc, irs_distance_comparat
                               void* stream);
 /* fetch_final_results / fetch_match_counters / fetch_all_match_ids
  * (distance_comparator.rs:748-893): final[q] = smallest matched entry,
- * 0xFFFFFFFE for an in-batch duplicate, 0xFFFFFFFF for no match. */
+ * 0xFFFFFFFE for an in-batch duplicate, 0xFFFFFFFF for no match.  In the
+ * asynchronous host mode the copies are only enqueued on party 0's stream
+ * (page-locked outputs, valid once an event recorded after the call has
+ * completed). */
 int irs_dc_fetch_final_results(irs_distance_comparator* dc, size_t n_queries, uint32_t* final_results,
                                uint32_t* match_counters, uint32_t* all_matches);
 

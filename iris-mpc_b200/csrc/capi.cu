@@ -1601,6 +1601,7 @@ int irs_dc_fetch_rows(irs_distance_comparator* dc, size_t first, size_t n, uint3
   cudaStream_t s = dm->streams[0];
   if (n) {
     CU(cudaMemcpyAsync(host, dc->bitmap + first * words, n * words * 4, cudaMemcpyDeviceToHost, s));
+    if (!dm->host_sync) return IRS_OK;  // rows valid once the stream passes the copy
     CU(cudaStreamSynchronize(s));
   }
   return check_device_error(dm);
@@ -1707,6 +1708,7 @@ int irs_dc_fetch_final_results(irs_distance_comparator* dc, size_t n_queries, ui
   if (match_counters) CU(cudaMemcpyAsync(match_counters, dc->match_counters, n_queries * 4, cudaMemcpyDeviceToHost, s));
   if (all_matches)
     CU(cudaMemcpyAsync(all_matches, dc->all_matches, n_queries * kMaxMatchesLen * 4, cudaMemcpyDeviceToHost, s));
+  if (!dm->host_sync) return IRS_OK;  // outputs valid once the stream passes the copies
   CU(cudaStreamSynchronize(s));
   return check_device_error(dm);
 }

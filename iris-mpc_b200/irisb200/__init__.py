@@ -696,6 +696,22 @@ class DistanceComparator:
     def clear_rows(self, first: int, n: int, stream=None) -> None:
         _check(lib().irs_dc_clear_rows(self.h, first, n, stream))
 
+    def row_words(self) -> int:
+        """u32 words per bitmap row (the stride of fetch_rows_into)."""
+        stride = _sz()
+        probe = np.zeros(1, np.uint32)
+        _check(lib().irs_dc_fetch_rows(self.h, 0, 0, _ptr(probe), 0, C.byref(stride)))
+        return stride.value
+
+    def fetch_rows_into(self, first: int, n: int, out: np.ndarray) -> None:
+        """Raw bitmap rows [first, first + n) into out [n][row_words()] u32
+        (page-locked, and read only after the stream has passed the call, in
+        the asynchronous host mode)."""
+        stride = _sz()
+        if out.dtype != np.uint32 or not out.flags.c_contiguous:
+            raise ValueError("fetch_rows_into needs a contiguous uint32 array")
+        _check(lib().irs_dc_fetch_rows(self.h, first, n, _ptr(out), out.size, C.byref(stride)))
+
     def fetch_rows(self, first: int, n: int, db_len: int) -> np.ndarray:
         """Bitmap rows [first, first+n) unpacked to [n][db_len] uint8."""
         stride = _sz()
@@ -740,6 +756,19 @@ class DistanceComparator:
         a = np.zeros((n_queries, MAX_MATCHES_LEN), np.uint32)
         _check(lib().irs_dc_fetch_final_results(self.h, n_queries, _ptr(f), _ptr(c), _ptr(a)))
         return f, c, a
+
+    def fetch_final_results_into(self, n_queries: int, final: np.ndarray, counters: np.ndarray,
+                                 matches: np.ndarray) -> None:
+        """irs_dc_fetch_final_results into caller-owned arrays (page-locked,
+        and read only after the stream has passed the call, in the
+        asynchronous host mode)."""
+        for a in (final, counters, matches):
+            if a.dtype != np.uint32 or not a.flags.c_contiguous:
+                raise ValueError("fetch_final_results_into needs contiguous uint32 arrays")
+        if final.size < n_queries or counters.size < n_queries or matches.shape[0] < n_queries or \
+                matches.shape[1] != MAX_MATCHES_LEN:
+            raise ValueError("output arrays too small")
+        _check(lib().irs_dc_fetch_final_results(self.h, n_queries, _ptr(final), _ptr(counters), _ptr(matches)))
 
     def close(self) -> None:
         if self.h:

@@ -27,7 +27,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import (IRIS_CODE_LENGTH, MASK_CODE_LENGTH, MAX_MATCHES_LEN, Circuits, DeviceManager, DistanceComparator,
-               Graph, ShareDB, dot_many)
+               Event, Graph, IrisError, PinnedArray, ShareDB, dot_many)
 
 MULTS = [1, 1, 1, 2, 2, 2]
 
@@ -58,6 +58,16 @@ class Result:
     mirror_matches: list = field(default_factory=list)  # matched entries of the mirrored variant
     reauth_match: bool | None = None
     reauth_mirror_match: bool | None = None
+
+
+@dataclass
+class Ticket:
+    """A submitted batch (BatchedEngine.submit); collect() returns its results."""
+    par: int
+    requests: list
+    uniq: list
+    reauth: list
+    results: list | None = None
 
 
 def full_face_mirror_attack(request: Request, result: Result) -> bool:
@@ -173,7 +183,11 @@ class BatchedEngine:
         for e in self.ce + self.me + self.sce + self.sme:
             e.use_batch_counter(True)
         circuits.use_batch_counter(True)
-        self.batch_id = 1
+        self._pin = None     # page-locked buffers, two sets (allocated on first use)
+        self._pinned = []    # their PinnedArray owners
+        self._events = None
+        self._inflight = [None, None]
+        self._par = 0
         self.graphs = {}
         self.tuned = {}
         self.autotune = autotune
@@ -214,7 +228,6 @@ class BatchedEngine:
         if g is None:
             g = self._capture(layout.n_slots, chunk)
             self.graphs[key] = g
-        self.dm.set_batch_counter(self.batch_id)
         g.launch(self.dm.stream(0))
 
     def _tune(self, layout: Layout):
@@ -240,6 +253,10 @@ class BatchedEngine:
 
     # -- one batch -----------------------------------------------------------
     def run(self, requests: list) -> list:
+        """Runs one batch and returns its results (submit + collect)."""
+        return self.collect(self.submit(requests))
+
+    def _variants(self, requests):
         uniq, reauth = [], []  # (request index, mirrored?)
         for i, r in enumerate(requests):
             dst = reauth if r.kind == "reauth" else uniq
@@ -248,79 +265,162 @@ class BatchedEngine:
                 dst.append((i, True))
         if len(uniq) > self.max_variants or len(reauth) > self.max_reauth:
             raise ValueError("batch exceeds the engine's variant capacity")
-        results = [Result() for _ in requests]
-        if uniq:
-            self._run_uniqueness(requests, uniq, results)
-        if reauth:
-            self._run_reauth(requests, reauth, results)
-        self.batch_id = (self.batch_id + 1) % (1 << 24) or 1
-        return results
+        return uniq, reauth
+
+    def _buffers(self):
+        """Two sets of page-locked host buffers, one per batch in flight."""
+        if self._pin is None:
+            def P(shape, dtype):
+                a = PinnedArray(shape, dtype)
+                self._pinned.append(a)
+                return a.array
+            nu, nr = self.max_variants, self.max_reauth
+            R, Rr = self.ce[0].query_length, self.sce[0].query_length
+            self._pin = [{
+                "ucode": P((3, nu, IRIS_CODE_LENGTH), np.uint16), "umask": P((3, nu, MASK_CODE_LENGTH), np.uint16),
+                "urows": P((R,), np.uint32),
+                "useg": (P((R // 32 + 1,), np.uint32), P((nu,), np.uint32), P((nu,), np.uint32)),
+                "final": P((nu,), np.uint32), "counters": P((nu,), np.uint32),
+                "matches": P((nu, MAX_MATCHES_LEN), np.uint32),
+                "rids": P((nr,), np.uint32),
+                "rcode": P((3, nr, IRIS_CODE_LENGTH), np.uint16), "rmask": P((3, nr, MASK_CODE_LENGTH), np.uint16),
+                "rrows": P((Rr,), np.uint32),
+                "rseg": (P((Rr // 32 + 1,), np.uint32), P((nr,), np.uint32), P((nr,), np.uint32)),
+                "rbits": P((nr, self.sdc.row_words()), np.uint32),
+            } for _ in range(2)]
+            self._events = [Event(), Event()]
+        return self._pin
 
     @staticmethod
-    def _bases(requests, variants):
-        """One base share per request (a mirrored variant reads its request's
-        base through the mirror bit): (code [3][n][12800], mask [3][n][6400],
-        base index per variant, mirrored flag per variant)."""
+    def _fill_bases(requests, variants, code, mask):
+        """One base share per request, written into code [3][*][12800] / mask
+        [3][*][6400] (a mirrored variant reads its request's base through the
+        mirror bit); returns (bases, base index per variant, mirrored flags)."""
         order = list(dict.fromkeys(i for i, _ in variants))
         index = {i: k for k, i in enumerate(order)}
-        code = np.empty((3, len(order), IRIS_CODE_LENGTH), np.uint16)
-        mask = np.empty((3, len(order), MASK_CODE_LENGTH), np.uint16)
         for k, i in enumerate(order):
             code[:, k] = requests[i].code
             mask[:, k] = requests[i].mask
-        return code, mask, [index[i] for i, _ in variants], [mir for _, mir in variants]
+        return len(order), [index[i] for i, _ in variants], [mir for _, mir in variants]
 
-    def _layout(self, requests, variants, base_of, mirrored) -> Layout:
-        return attach_bases(pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants]), base_of, mirrored)
+    def _stage(self, requests, variants, code, mask, rows, seg, cap: int, pad: bool):
+        """Bases, row table and segment table of one pass in the page-locked
+        buffers; returns (layout, bases, rows used, segments used)."""
+        nb, base_of, mirrored = self._fill_bases(requests, variants, code, mask)
+        layout = attach_bases(pack([list(centred_rotations(requests[i].n_rot)) for i, _ in variants]),
+                              base_of, mirrored)
+        if pad:
+            layout = pad_rows(layout, cap)
+        if layout.n_rows > rows.size:
+            raise ValueError("batch exceeds the engine's query-row capacity")
+        rows[: layout.n_rows] = layout.row_desc
+        ss, sq, sm = seg
+        ns, nq = layout.seg_start.size, layout.seg_query.size
+        ss[:ns], sq[:nq], sm[:nq] = layout.seg_start, layout.seg_query, layout.seg_mask
+        return layout, nb, layout.n_rows, (ns, nq)
 
-    def _run_uniqueness(self, requests, variants, results):
-        code, mask, base_of, mirrored = self._bases(requests, variants)
-        layout = pad_rows(self._layout(requests, variants, base_of, mirrored), self.ce[0].query_length)
-        for p in range(3):
-            self.ce[p].query_upload_rows(code[p], layout.row_desc)
-            self.me[p].query_upload_rows(mask[p], layout.row_desc)
-        self.dc.set_segments(layout.seg_start, layout.seg_query, layout.seg_mask)
-        tile, chunk = self._tune(layout)
-        self._run_db_pass(layout, tile, chunk)
-        final, counters, allm = self.dc.fetch_final_results(len(variants))
-        for v, (i, mir) in enumerate(variants):
-            ids = sorted(allm[v, :min(int(counters[v]), MAX_MATCHES_LEN)].tolist())
+    def submit(self, requests: list) -> "Ticket":
+        """Prepares one batch in page-locked buffers and enqueues its device
+        work (the DB pass and the reauth pass, then the result copies),
+        returning without waiting; collect() returns its results.  Two
+        batches can be in flight, so the host prepares batch k+1 while the
+        GPU runs batch k; submitting a third first collects the batch whose
+        buffers it reuses."""
+        uniq, reauth = self._variants(requests)
+        par = self._par
+        if self._inflight[par] is not None:
+            self.collect(self._inflight[par])
+        buf = self._buffers()[par]
+        if uniq:
+            ulay, unb, urows, (uns, unq) = self._stage(requests, uniq, buf["ucode"], buf["umask"], buf["urows"],
+                                                       buf["useg"], self.ce[0].query_length, pad=True)
+        if reauth:
+            rlay, rnb, rrows, (rns, rnq) = self._stage(requests, reauth, buf["rcode"], buf["rmask"], buf["rrows"],
+                                                       buf["rseg"], self.sce[0].query_length, pad=False)
+            ids = buf["rids"][: len(reauth)]
+            ids[:] = [requests[i].target for i, _ in reauth]
+        self.dm.set_host_sync(False)
+        try:
+            self.dm.advance_batch_counter()  # fresh ChaCha batch id for both passes
+            if uniq:
+                rt = buf["urows"][:urows]
+                for p in range(3):
+                    self.ce[p].query_upload_rows(buf["ucode"][p, :unb], rt)
+                    self.me[p].query_upload_rows(buf["umask"][p, :unb], rt)
+                ss, sq, sm = buf["useg"]
+                self.dc.set_segments(ss[:uns], sq[:unq], sm[:unq])
+                tile, chunk = self._tune(ulay)  # times candidates (synchronously) once per padded size
+                self._run_db_pass(ulay, tile, chunk)
+                n = len(uniq)
+                self.dc.fetch_final_results_into(n, buf["final"][:n], buf["counters"][:n], buf["matches"][:n])
+            if reauth:
+                n = len(reauth)
+                for p in range(3):
+                    self.sce[p].gather_records(self.ce[p], ids)
+                    self.sme[p].gather_records(self.me[p], ids)
+                rt = buf["rrows"][:rrows]
+                for p in range(3):
+                    self.sce[p].query_upload_rows(buf["rcode"][p, :rnb], rt)
+                    self.sme[p].query_upload_rows(buf["rmask"][p, :rnb], rt)
+                for e in self.sce + self.sme:
+                    e.set_tile(0)
+                self.sdc.reset()
+                ss, sq, sm = buf["rseg"]
+                self.sdc.set_segments(ss[:rns], sq[:rnq], sm[:rnq])
+                dot_many(self.sce + self.sme, MULTS, 0, n)
+                self.sdc.compare_threshold_open_prepared(self.c, self.sce, self.sme, 0, n, self.threshold_a)
+                self.sdc.fetch_rows_into(0, n, buf["rbits"][:n])
+            self._events[par].record(self.dm.stream(0))
+        except BaseException:
+            self.dm.synchronize()  # nothing may still read the buffers
+            raise
+        finally:
+            self.dm.set_host_sync(True)
+        t = Ticket(par, requests, uniq, reauth)
+        self._inflight[par] = t
+        self._par ^= 1
+        return t
+
+    def collect(self, ticket: "Ticket") -> list:
+        """Waits for a submitted batch and returns its results (per request:
+        sorted DB matches of each uniqueness orientation, the match bit of
+        each reauth orientation against its target)."""
+        if ticket.results is not None:
+            return ticket.results
+        self._events[ticket.par].synchronize()
+        self._inflight[ticket.par] = None
+        code = self.dm.error_code()
+        if code:
+            raise IrisError(code, "a kernel reported a device error during a batched launch")
+        buf = self._pin[ticket.par]
+        results = [Result() for _ in ticket.requests]
+        counters, matches = buf["counters"], buf["matches"]
+        for v, (i, mir) in enumerate(ticket.uniq):
+            ids = sorted(matches[v, :min(int(counters[v]), MAX_MATCHES_LEN)].tolist())
             if mir:
                 results[i].mirror_matches = ids
             else:
                 results[i].matches = ids
-
-    def _run_reauth(self, requests, variants, results):
-        ids = np.array([requests[i].target for i, _ in variants], np.uint32)
-        for p in range(3):
-            self.sce[p].gather_records(self.ce[p], ids)
-            self.sme[p].gather_records(self.me[p], ids)
-        code, mask, base_of, mirrored = self._bases(requests, variants)
-        layout = self._layout(requests, variants, base_of, mirrored)
-        for p in range(3):
-            self.sce[p].query_upload_rows(code[p], layout.row_desc)
-            self.sme[p].query_upload_rows(mask[p], layout.row_desc)
-        for e in self.sce + self.sme:
-            e.set_tile(0)
-        n = len(variants)
-        self.dm.set_batch_counter(self.batch_id)
-        self.sdc.reset()
-        self.sdc.set_segments(layout.seg_start, layout.seg_query, layout.seg_mask)
-        dot_many(self.sce + self.sme, MULTS, 0, n)
-        self.sdc.compare_threshold_open_prepared(self.c, self.sce, self.sme, 0, n, self.threshold_a)
-        self.dm.synchronize()
-        from . import bitmap_get
-        bm = bitmap_get(self.sdc.fetch_bitmap(n, n), n, n)
-        for v, (i, mir) in enumerate(variants):
-            hit = bool(bm[v, v])  # variant v against its own target (subset record v)
+        bits = buf["rbits"]
+        for v, (i, mir) in enumerate(ticket.reauth):
+            hit = bool((int(bits[v, v // 32]) >> (v % 32)) & 1)  # variant v against subset record v
             if mir:
                 results[i].reauth_mirror_match = hit
             else:
                 results[i].reauth_match = hit
+        ticket.results = results
+        return results
 
     def close(self) -> None:
+        self.dm.synchronize()
         for g in self.graphs.values():
             g.close()
         self.graphs.clear()
         for o in self.sce + self.sme + [self.dc, self.sdc]:
             o.close()
+        for a in self._pinned:
+            a.free()
+        for e in self._events or []:
+            e.close()
+        self._pinned = []
+        self._pin = self._events = None

@@ -121,3 +121,29 @@ def test_batched_equals_plain_slots(dm, oracle, setup):
     finally:
         eng.close()
         c.close()
+
+
+def test_pipelined_batches_match_one_at_a_time(dm, oracle, setup):
+    """Two different batches in flight at once (submit, submit, collect,
+    collect, and a third submit that collects the batch whose buffers it
+    reuses) give the same results as the same batches run one at a time."""
+    s = setup
+    c = irisb200.Circuits(dm, W.SEEDS)
+    eng = BatchedEngine(dm, s["ce"], s["me"], c, max_variants=32, max_reauth=8, threshold_a=A)
+    try:
+        def req(q, n, mir, k="uniqueness", t=-1):
+            return Request(code=s["qc"][:, q], mask=s["qm"][:, q], n_rot=n, mirrored=mir, kind=k, target=t)
+        batch_a = [req(0, 31, True), req(3, 16, False), req(6, 31, False, "reauth", 1000), req(1, 1, True)]
+        batch_b = [req(3, 31, True), req(8, 1, False, "reauth", 333), req(2, 31, False), req(5, 16, True),
+                   req(0, 16, False, "reauth", 5)]
+        alone_a, alone_b = eng.run(batch_a), eng.run(batch_b)
+        ta, tb = eng.submit(batch_a), eng.submit(batch_b)
+        tc = eng.submit(batch_a)  # reuses batch a's buffers: collects it first
+        assert ta.results is not None
+        for got, want in ((eng.collect(ta), alone_a), (eng.collect(tb), alone_b), (eng.collect(tc), alone_a)):
+            assert got == want
+        assert 5 in alone_a[0].matches and 64 in alone_b[0].matches
+        assert alone_a[2].reauth_match is True
+    finally:
+        eng.close()
+        c.close()
