@@ -48,3 +48,18 @@ def test_comparisons_and_latency_summary():
     assert st["completed"] == 4
     assert abs(st["p50_ms"] - 300.0) < 1e-6 and abs(st["max_ms"] - 500.0) < 1e-6
     assert abs(st["comparisons_per_s"] - (2000 + 1 + 2002) / 1.0) < 1e-6
+
+
+def test_measured_peaks_parsing(tmp_path, monkeypatch):
+    """MEASURED_PEAKS.json figures are read as numbers or {"value": n};
+    absent or malformed figures come back as None."""
+    import json
+    import bench
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.measured_peaks()["present"] is False
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps(
+        {"hbm_gbs": 6540.5, "bf16_tflops": {"value": 1590}, "bf16_tflops_sustained": "n/a"}))
+    mp = bench.measured_peaks()
+    assert mp == {"hbm_gbs": 6540.5, "bf16_tflops": 1590.0, "bf16_tflops_sustained": None, "present": True}
+    (tmp_path / "MEASURED_PEAKS.json").write_text("{not json")
+    assert bench.measured_peaks()["hbm_gbs"] is None
