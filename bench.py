@@ -456,27 +456,30 @@ def run_ours(args):
         n_reauth = sum(2 if r.mirrored else 1 for r in reqs if r.kind == "reauth")
         eng = BatchedEngine(dm, ce, me, c, max_variants=max(64, n_var), max_reauth=max(16, n_reauth),
                             threshold_a=A, seeds=seeds, autotune=True)
-        lat_alone = []  # one batch at a time: warm-up runs after the first (which autotunes and captures)
-        for k in range(max(3, args.warmup)):
-            ts = time.perf_counter()
+        for _ in range(max(2, args.warmup)):  # the first autotunes and captures
             eng.run(reqs)
-            if k:
-                lat_alone.append((time.perf_counter() - ts) * 1e3)
         dm.synchronize()
         blat = []
         with clk.mark():
             tb = time.perf_counter()
-            pend = None  # (ticket, submit time): two batches in flight
-            for _ in range(args.steps):
+            for _ in range(args.steps):  # one batch at a time
                 ts = time.perf_counter()
-                ticket = eng.submit(reqs)
-                if pend:
-                    bres = eng.collect(pend[0])
-                    blat.append((time.perf_counter() - pend[1]) * 1e3)
-                pend = (ticket, ts)
-            bres = eng.collect(pend[0])
-            blat.append((time.perf_counter() - pend[1]) * 1e3)
+                bres = eng.run(reqs)
+                blat.append((time.perf_counter() - ts) * 1e3)
             tb = time.perf_counter() - tb
+        plat = []
+        tp = time.perf_counter()
+        pend = None  # (ticket, submit time): two batches in flight
+        for _ in range(args.steps):
+            ts = time.perf_counter()
+            ticket = eng.submit(reqs)
+            if pend:
+                eng.collect(pend[0])
+                plat.append((time.perf_counter() - pend[1]) * 1e3)
+            pend = (ticket, ts)
+        eng.collect(pend[0])
+        plat.append((time.perf_counter() - pend[1]) * 1e3)
+        tp = time.perf_counter() - tp
         bcomp = sum(comparisons_of(r, M) for r in reqs)
         rows = sum(r.n_rot * (2 if r.mirrored else 1) for r in reqs if r.kind == "uniqueness")
         tuned = {str(k): list(v) for k, v in eng.tuned.items()}
@@ -493,20 +496,20 @@ def run_ours(args):
         batched = {
             "value": bcomp * args.steps / tb, "unit": UNIT,
             "vs_plain_e2e": (bcomp * args.steps / tb) / e2e_value,
-            "latency_ms": {"p50": sorted(blat)[len(blat) // 2], "p99": max(blat),
-                           "what": "submit to collect with two batches in flight (includes the wait for the "
-                                   "batch ahead)"},
-            "latency_alone_ms": {"p50": sorted(lat_alone)[len(lat_alone) // 2], "p99": max(lat_alone),
-                                 "what": "one batch at a time through BatchedEngine.run"},
+            "latency_ms": {"p50": sorted(blat)[len(blat) // 2], "p99": max(blat)},
+            "pipelined": {"value": bcomp * args.steps / tp, "unit": UNIT,
+                          "latency_ms": {"p50": sorted(plat)[len(plat) // 2], "p99": max(plat)},
+                          "what": "the same batches with two in flight (BatchedEngine.submit / collect: the "
+                                  "host prepares batch k+1 while the GPU runs batch k); latency = submit to "
+                                  "collect, including the wait for the batch ahead"},
             "config": {"workload": f"batched uneven launches: {nb} requests per batch, rotations 1/16/31, "
                                    "50% mirrored, 80% uniqueness (full DB) / 20% reauth (one target)",
                        "uniqueness_orientations": n_var, "reauth_orientations": n_reauth,
                        "uniqueness_query_rows": rows, "packed_rows": lay.n_rows, "comparisons_per_batch": bcomp,
                        "autotuned_tile_chunk": tuned,
-                       "timing": "host wall clock over the steps, batches pipelined two deep through "
-                                 "BatchedEngine.submit / collect (the host prepares batch k+1 while the GPU runs "
-                                 "batch k); latency = submit to collect of each batch (H2D of the shares, graph "
-                                 "replay of the DB pass, reauth subset pass, D2H of the match lists)"},
+                       "timing": "host wall clock per batch through BatchedEngine.run, one batch at a time "
+                                 "(H2D of the shares, graph replay of the DB pass, reauth subset pass, D2H of "
+                                 "the match lists)"},
             "planted_matches_found": f"{planted_hits}/{planted_window}",
             "planted_note": f"of the {planted_uniq} planted uniqueness requests, {planted_window} have the "
                             "planted rotation inside their rotation window",
