@@ -307,7 +307,35 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
       }
       lift_carries(M, wr, c1, c2);
     }
+    // Party p's lift correction C_p[j] = inject(c1)_p[j] + 2 inject(c2)_p[j]
+    // (mod 2^16), two elements per word.  The injections run as rolled loops
+    // over a small per-thread array: one copy of their code instead of 64
+    // unrolled ones keeps the kernel's straight-line code (executed once per
+    // word) small enough for the instruction cache.
+    uint32_t corr[3][16];
+    wr.load(6);
+#pragma unroll 1
+    for (int i = 0; i < 16; i++) {
+      uint32_t a[3], b[3];
+      inject_bit(c1, 2 * i, wr.ks, a[0], a[1], a[2]);
+      inject_bit(c1, 2 * i + 1, wr.ks, b[0], b[1], b[2]);
+#pragma unroll
+      for (int p = 0; p < 3; p++) corr[p][i] = a[p] | (b[p] << 16);
+    }
+    wr.load(7);
+#pragma unroll 1
+    for (int i = 0; i < 16; i++) {
+      uint32_t a[3], b[3];
+      inject_bit(c2, 2 * i, wr.ks, a[0], a[1], a[2]);
+      inject_bit(c2, 2 * i + 1, wr.ks, b[0], b[1], b[2]);
+#pragma unroll
+      for (int p = 0; p < 3; p++) {
+        const uint32_t w = corr[p][i];
+        corr[p][i] = ((w + 2u * a[p]) & 0xFFFFu) | (((w >> 16) + 2u * b[p]) << 16);
+      }
+    }
     // X_p = (mask_p - A1_p<<16 - A2_p<<17) * A - code_p<<16 - [p == 0]
+    //     = mask_p * A - ((C_p * A + code_p) << 16) - [p == 0]   (mod 2^32)
 #pragma unroll
     for (int p = 0; p < 3; p++) {
       uint32_t wm[16], wc[16];
@@ -317,26 +345,9 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
       for (int j = 0; j < 32; j++) {
         const uint32_t m = (wm[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
         const uint32_t c = (wc[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
-        X[p][j] = m * threshold_a - (c << 16) - (p == 0 ? 1u : 0u);
+        const uint32_t cr = (corr[p][j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
+        X[p][j] = m * threshold_a - ((cr * threshold_a + c) << 16) - (p == 0 ? 1u : 0u);
       }
-    }
-    wr.load(6);
-#pragma unroll
-    for (int j = 0; j < 32; j++) {
-      uint32_t A0, A1, A2;
-      inject_bit(c1, j, wr.ks, A0, A1, A2);
-      X[0][j] -= (A0 << 16) * threshold_a;
-      X[1][j] -= (A1 << 16) * threshold_a;
-      X[2][j] -= (A2 << 16) * threshold_a;
-    }
-    wr.load(7);
-#pragma unroll
-    for (int j = 0; j < 32; j++) {
-      uint32_t A0, A1, A2;
-      inject_bit(c2, j, wr.ks, A0, A1, A2);
-      X[0][j] -= (A0 << 17) * threshold_a;
-      X[1][j] -= (A1 << 17) * threshold_a;
-      X[2][j] -= (A2 << 17) * threshold_a;
     }
   } else {
     // extract_msb with the lifted mask and corrections at zero:

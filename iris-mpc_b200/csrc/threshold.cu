@@ -184,8 +184,8 @@ cudaError_t launch_threshold_bitmap(const ThresholdParams& P, cudaStream_t strea
   if (P.n_entries == 0 || P.n_slots == 0) return cudaSuccess;
   const uint64_t warps = (uint64_t)((P.n_entries + 31) / 32) * P.n_slots;
   // Resident warps per SM the kernel's registers are sized for: 12 (3 per
-  // SM sub-partition: 168 registers with a 48-byte spill) measured 4-6%
-  // faster than 8 (195 registers, no spill) on 512K-entry batches.  Other
+  // SM sub-partition, 168-register cap) measured 2-6% faster than 8 on
+  // 512K-entry batches.  Other
   // counts give the same register cap as one of these two, since each
   // sub-partition holds a quarter of the register file.
   // IRS_THRESHOLD_WARPS_PER_SM=8 selects the other variant for tuning runs.
