@@ -173,3 +173,18 @@ def test_submit_rejects_oversized_batches(monkeypatch):
         e.submit([Request(code=z[0], mask=z[1], n_rot=31, mirrored=True) for _ in range(6)])
     assert e._inflight == [None, None]
     assert not any(isinstance(c, tuple) for c in dm.calls)  # failed before any device work
+
+
+def test_submit_edge_batches(monkeypatch):
+    """An empty batch, a reauth-only batch and a uniqueness-only batch each
+    complete; only the passes a batch needs are enqueued."""
+    from irisb200.batched import Request
+    e, dm = _fake_engine(monkeypatch)
+    z = np.zeros((3, 12800), np.uint16), np.zeros((3, 6400), np.uint16)
+    assert e.run([]) == []
+    assert "compare_threshold_open_prepared" not in e.sdc.calls and not e.graphs
+    res = e.run([Request(code=z[0], mask=z[1], n_rot=1, kind="reauth", target=3)])
+    assert res[0].reauth_match is True and res[0].matches == [] and not e.graphs
+    res = e.run([Request(code=z[0], mask=z[1], n_rot=16)])
+    assert res[0].matches == [100] and res[0].reauth_match is None and e.graphs
+    e.close()
