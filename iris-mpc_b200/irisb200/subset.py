@@ -15,6 +15,15 @@ Here the subset is gathered device-to-device into a small engine per party
 (irs_sharedb_gather_records), the batch runs in 32-row slots against it, and
 the compacted match lists (irs_dc_take_rows) are mapped back through the id
 list on the host.
+
+The reference also records, for every opened (query rotation, subset entry)
+match, the signed rotation (-15..15) next to the DB index
+(openResultsWithIndexMapping, kernel.cu:118-151; get_partial_results_with_
+rotations, distance_comparator.rs:650-711), and the actor lists the matching
+rotations of each partial match (map_rotation_indices_to_db_ids_per_query,
+actor.rs:2859-2883).  run_with_rotations does the same from the comparator's
+distance capture, whose records carry the query row (32 * query + rotation
+index) of each opened match.
 """
 from __future__ import annotations
 
@@ -31,7 +40,7 @@ class SubsetPass:
     gathered subset of the DB held by code_engines / mask_engines."""
 
     def __init__(self, dm, code_engines, mask_engines, circuits, max_queries: int = 64,
-                 max_subset: int = DB_CHUNK_SIZE, seeds=None):
+                 max_subset: int = DB_CHUNK_SIZE, seeds=None, rotations: bool = False):
         self.dm = dm
         self.ce, self.me = list(code_engines), list(mask_engines)
         self.c = circuits
@@ -44,19 +53,39 @@ class SubsetPass:
         for e in self.sce + self.sme:
             e.alloc_db(max_subset)
         self.dc = DistanceComparator(dm, max_queries, max(max_subset, 64), match_list_cap=1 << 12)
+        # rotation records: as the reference, up to MAX_MATCHES_LEN per query row
+        self.rot_cap = MAX_MATCHES_LEN * 31 * max_queries if rotations else 0
+        self.rotations_lost = 0
+        if rotations:
+            self.dc.enable_distance_capture(self.rot_cap)
 
     def run(self, code_base: np.ndarray, mask_base: np.ndarray, ids, threshold_a: int):
         """code_base [3][nq][12800] / mask_base [3][nq][6400]: the batch's
         preprocessed base shares; ids: DB indices of the subset.  Returns, per
         query, the sorted DB indices it matches among `ids` (at most
         MAX_MATCHES_LEN per subset chunk, as the reference's lists)."""
+        return self._run(code_base, mask_base, ids, threshold_a, False)[0]
+
+    def run_with_rotations(self, code_base: np.ndarray, mask_base: np.ndarray, ids, threshold_a: int):
+        """run() plus, per query, one sorted list of the matching signed
+        rotations (-15..15, 0 = centre) for each returned DB index
+        (partial_match_rotation_indices).  Needs rotations=True at
+        construction; self.rotations_lost counts records beyond the capture
+        capacity (the reference drops them too)."""
+        if not self.rot_cap:
+            raise ValueError("construct the subset pass with rotations=True")
+        return self._run(code_base, mask_base, ids, threshold_a, True)
+
+    def _run(self, code_base, mask_base, ids, threshold_a: int, want_rot: bool):
         nq = code_base.shape[1]
         if nq > self.max_queries:
             raise ValueError("too many queries for this subset pass")
         ids = np.unique(np.asarray(ids, np.int64)).astype(np.uint32)
         out = [[] for _ in range(nq)]
+        rot = [dict() for _ in range(nq)]  # query -> DB index -> rotations
+        self.rotations_lost = 0
         if ids.size == 0:
-            return out
+            return out, [[] for _ in range(nq)]
         slots = [(j, 0, 31, j) for j in range(nq)]
         for p in range(3):
             self.sce[p].query_upload_slots(code_base[p], slots)
@@ -74,7 +103,15 @@ class SubsetPass:
             for q in range(nq):
                 k = min(int(counts[q]), MAX_MATCHES_LEN)
                 out[q].extend(chunk[pos[q, :k]].tolist())  # subset position -> DB index
-        return [sorted(x) for x in out]
+            if self.rot_cap:
+                entry, row, _, _, total = self.dc.fetch_distances(self.rot_cap, reset=True)
+                self.rotations_lost += max(0, total - self.rot_cap)
+                if want_rot:
+                    for e, r in zip(entry.tolist(), row.tolist()):
+                        q, ri = divmod(r, 32)  # slot q holds query q's 31 rotations
+                        rot[q].setdefault(int(chunk[e]), []).append(ri - 15)
+        out = [sorted(x) for x in out]
+        return out, [[sorted(rot[q].get(e, [])) for e in out[q]] for q in range(nq)]
 
     def close(self) -> None:
         for o in self.sce + self.sme + [self.dc]:

@@ -73,3 +73,44 @@ def test_two_stage_equals_full_scan(dm, oracle):
         c.close()
         for e in left[0] + left[1] + right[0] + right[1]:
             e.close()
+
+
+def _rotation_hits(oracle, cs, ms, qc, qm, entries, threshold_a):
+    """{entry: sorted signed rotations (-15..15) at which the query matches}
+    on the CPU: per-party dots of all 31 rotation rows, summed, thresholded."""
+    entries = np.asarray(entries)
+    code = 0
+    mask = 0
+    for p in range(3):
+        rc = np.stack([oracle.rotate_share(qc[p], r) for r in range(31)])
+        rm = np.stack([oracle.rotate_share(qm[p], r) for r in range(31)])
+        code = code + oracle.dot_u16(rc, cs[p][entries]).astype(np.uint64)
+        mask = mask + 2 * oracle.dot_u16(rm, ms[p][entries]).astype(np.uint64)
+    hit = oracle.match_predicate(code % 65536, mask % 65536, threshold_a)  # [31][n]
+    return {int(e): [r - 15 for r in range(31) if hit[r, k]] for k, e in enumerate(entries) if hit[:, k].any()}
+
+
+def test_subset_rotation_indices(dm, oracle):
+    """partial_match_rotation_indices: for every DB index a query matches in
+    the subset pass, the signed rotations that matched, == the CPU path.
+    Planted copies shifted by r match around rotation -r; a query planted
+    twice from one entry covers two DB indices."""
+    ce, me, cs, ms, qc, qm = _engines(dm, oracle, 0xC0FFEE, 33, {0: (11, 0), 2: (500, 5), 4: (1200, -7), 7: (11, 3)})
+    c = irisb200.Circuits(dm, W.SEEDS)
+    sp = SubsetPass(dm, ce, me, c, max_queries=NQ, max_subset=4, rotations=True)
+    try:
+        cand = [3, 11, 12, 500, 777, 1200, 1499]
+        ids, rots = sp.run_with_rotations(qc, qm, cand, irisb200.THRESHOLD_A)
+        assert sp.rotations_lost == 0
+        for q in range(NQ):
+            want = _rotation_hits(oracle, cs, ms, qc[:, q], qm[:, q], cand, irisb200.THRESHOLD_A)
+            assert ids[q] == sorted(want), f"query {q}"
+            assert rots[q] == [want[e] for e in ids[q]], f"query {q}"
+        assert 11 in ids[0] and 500 in ids[2] and 1200 in ids[4] and 11 in ids[7]
+        assert all(len(r) >= 1 for q in range(NQ) for r in rots[q])
+        assert sp.run(qc, qm, cand, irisb200.THRESHOLD_A) == ids  # run() == the ids of run_with_rotations
+    finally:
+        sp.close()
+        c.close()
+        for e in ce + me:
+            e.close()
