@@ -56,6 +56,7 @@ class SubsetPass:
         # rotation records: as the reference, up to MAX_MATCHES_LEN per query row
         self.rot_cap = MAX_MATCHES_LEN * 31 * max_queries if rotations else 0
         self.rotations_lost = 0
+        self.match_counts = np.zeros(0, np.int64)
         if rotations:
             self.dc.enable_distance_capture(self.rot_cap)
 
@@ -84,6 +85,9 @@ class SubsetPass:
         out = [[] for _ in range(nq)]
         rot = [dict() for _ in range(nq)]  # query -> DB index -> rotations
         self.rotations_lost = 0
+        # partial_match_counters: every match of the query, also those past
+        # the MAX_MATCHES_LEN ids a chunk returns
+        self.match_counts = np.zeros(nq, np.int64)
         if ids.size == 0:
             return out, [[] for _ in range(nq)]
         slots = [(j, 0, 31, j) for j in range(nq)]
@@ -100,6 +104,7 @@ class SubsetPass:
             dot_many(self.sce + self.sme, MULTS, 0, n)
             self.dc.compare_threshold_open(self.c, self.sce, self.sme, 0, n, nq, threshold_a)
             counts, pos = self.dc.take_rows(np.arange(nq, dtype=np.uint32), n, clear=True)
+            self.match_counts += counts[:nq].astype(np.int64)
             for q in range(nq):
                 k = min(int(counts[q]), MAX_MATCHES_LEN)
                 out[q].extend(chunk[pos[q, :k]].tolist())  # subset position -> DB index

@@ -109,6 +109,7 @@ def test_subset_rotation_indices(dm, oracle):
         assert 11 in ids[0] and 500 in ids[2] and 1200 in ids[4] and 11 in ids[7]
         assert all(len(r) >= 1 for q in range(NQ) for r in rots[q])
         assert sp.run(qc, qm, cand, irisb200.THRESHOLD_A) == ids  # run() == the ids of run_with_rotations
+        assert sp.match_counts.tolist() == [len(x) for x in ids]  # partial_match_counters
     finally:
         sp.close()
         c.close()
