@@ -58,21 +58,30 @@ __host__ __device__ __noinline__
 #else
 static
 #endif
-void chacha12_x3(const ChaChaKey* key, uint64_t counter, uint64_t nonce, uint32_t* ks) {
+void chacha12_x3(const uint32_t* pre, uint32_t ctr_lo, uint32_t* ks) {
 #pragma unroll 1
-  for (int s = 0; s < 3; s++) chacha_block<12>(key[s], counter, nonce, ks + 16 * s);
+  for (int s = 0; s < 3; s++) chacha12_block_prepared(pre + 24 * s, ctr_lo, ks + 16 * s);
 }
 
 // Keystream of one word: the current block of each of the three streams.
+// The eight blocks of a word share their counter's high word (the low word
+// of block 0's counter is a multiple of 8), so round 1's constant columns
+// are prepared once per word and stream (chacha_prepare).
 struct WordRand {
   ChaChaKey key[3];
   uint64_t nonce;
   uint64_t base;  // counter of block 0 of this word
   uint32_t ks[3][16];
   int block;
+  bool prepared = false;
+  alignas(16) uint32_t pre[3][24];
   IRS_HD void load(int b) {
     block = b;
-    chacha12_x3(key, base + (uint64_t)b, nonce, &ks[0][0]);
+    if (!prepared) {
+      for (int s = 0; s < 3; s++) chacha_prepare(key[s], (uint32_t)(base >> 32), nonce, pre[s]);
+      prepared = true;
+    }
+    chacha12_x3(&pre[0][0], (uint32_t)(base + (uint64_t)b), &ks[0][0]);
   }
 };
 

@@ -93,6 +93,50 @@ IRS_HD void chacha_block(const ChaChaKey& key, uint64_t counter, uint64_t nonce,
   out[12] = x12 + (uint32_t)counter; out[13] = x13 + (uint32_t)(counter >> 32);
   out[14] = x14 + (uint32_t)nonce; out[15] = x15 + (uint32_t)(nonce >> 32);
 }
+
+// Round 1's column quarter rounds 1..3 read only the key, the high counter
+// word and the nonce, so blocks that share those (the eight blocks of one
+// circuit word: their counters never carry into the high word) share them.
+// pre[24] = key[8] | ctr_hi | nonce_lo | nonce_hi | 0 | the twelve words of
+// columns 1..3 after round 1 (x1 x5 x9 x13, x2 x6 x10 x14, x3 x7 x11 x15).
+IRS_HD void chacha_prepare(const ChaChaKey& key, uint32_t ctr_hi, uint64_t nonce, uint32_t pre[24]) {
+  for (int i = 0; i < 8; i++) pre[i] = key.k[i];
+  pre[8] = ctr_hi;
+  pre[9] = (uint32_t)nonce;
+  pre[10] = (uint32_t)(nonce >> 32);
+  pre[11] = 0;
+  uint32_t x1 = 0x3320646eu, x5 = key.k[1], x9 = key.k[5], x13 = ctr_hi;
+  uint32_t x2 = 0x79622d32u, x6 = key.k[2], x10 = key.k[6], x14 = pre[9];
+  uint32_t x3 = 0x6b206574u, x7 = key.k[3], x11 = key.k[7], x15 = pre[10];
+  IRS_QR(x1, x5, x9, x13) IRS_QR(x2, x6, x10, x14) IRS_QR(x3, x7, x11, x15)
+  pre[12] = x1; pre[13] = x5; pre[14] = x9; pre[15] = x13;
+  pre[16] = x2; pre[17] = x6; pre[18] = x10; pre[19] = x14;
+  pre[20] = x3; pre[21] = x7; pre[22] = x11; pre[23] = x15;
+}
+
+// ChaCha12 block with counter (pre's ctr_hi << 32 | ctr_lo): the same
+// keystream as chacha_block<12>, starting from the prepared columns.
+// `pre` is 16-byte aligned.
+IRS_HD void chacha12_block_prepared(const uint32_t* pre, uint32_t ctr_lo, uint32_t out[16]) {
+  const uint4* q = reinterpret_cast<const uint4*>(pre);
+  const uint4 k0 = q[0], k1 = q[1], cn = q[2], c1 = q[3], c2 = q[4], c3 = q[5];
+  const uint32_t s0 = 0x61707865u, s1 = 0x3320646eu, s2 = 0x79622d32u, s3 = 0x6b206574u;
+  uint32_t x0 = s0, x4 = k0.x, x8 = k1.x, x12 = ctr_lo;
+  IRS_QR(x0, x4, x8, x12)
+  uint32_t x1 = c1.x, x5 = c1.y, x9 = c1.z, x13 = c1.w;
+  uint32_t x2 = c2.x, x6 = c2.y, x10 = c2.z, x14 = c2.w;
+  uint32_t x3 = c3.x, x7 = c3.y, x11 = c3.z, x15 = c3.w;
+  IRS_QR(x0, x5, x10, x15) IRS_QR(x1, x6, x11, x12) IRS_QR(x2, x7, x8, x13) IRS_QR(x3, x4, x9, x14)
+#pragma unroll
+  for (int i = 1; i < 6; i++) {
+    IRS_QR(x0, x4, x8, x12) IRS_QR(x1, x5, x9, x13) IRS_QR(x2, x6, x10, x14) IRS_QR(x3, x7, x11, x15)
+    IRS_QR(x0, x5, x10, x15) IRS_QR(x1, x6, x11, x12) IRS_QR(x2, x7, x8, x13) IRS_QR(x3, x4, x9, x14)
+  }
+  out[0] = x0 + s0; out[1] = x1 + s1; out[2] = x2 + s2; out[3] = x3 + s3;
+  out[4] = x4 + k0.x; out[5] = x5 + k0.y; out[6] = x6 + k0.z; out[7] = x7 + k0.w;
+  out[8] = x8 + k1.x; out[9] = x9 + k1.y; out[10] = x10 + k1.z; out[11] = x11 + k1.w;
+  out[12] = x12 + ctr_lo; out[13] = x13 + cn.x; out[14] = x14 + cn.y; out[15] = x15 + cn.z;
+}
 #undef IRS_QR
 #undef IRS_ROT16
 #undef IRS_ROT8
