@@ -65,7 +65,7 @@ void chacha12_x3(const uint32_t* pre, uint32_t ctr_lo, uint32_t* ks) {
 
 // Keystream of one word: the current block of each of the three streams.
 // The eight blocks of a word share their counter's high word (the low word
-// of block 0's counter is a multiple of 8), so round 1's constant columns
+// of block 0's counter is a multiple of 8), so the first ChaCha round's constant columns
 // are prepared once per word and stream (chacha_prepare).
 struct WordRand {
   ChaChaKey key[3];

@@ -94,11 +94,11 @@ IRS_HD void chacha_block(const ChaChaKey& key, uint64_t counter, uint64_t nonce,
   out[14] = x14 + (uint32_t)nonce; out[15] = x15 + (uint32_t)(nonce >> 32);
 }
 
-// Round 1's column quarter rounds 1..3 read only the key, the high counter
-// word and the nonce, so blocks that share those (the eight blocks of one
-// circuit word: their counters never carry into the high word) share them.
+// The first ChaCha round's column quarter rounds 1..3 read only the key, the
+// high counter word and the nonce, so blocks that share those (the eight blocks
+// of one circuit word: their counters never carry into the high word) share them.
 // pre[24] = key[8] | ctr_hi | nonce_lo | nonce_hi | 0 | the twelve words of
-// columns 1..3 after round 1 (x1 x5 x9 x13, x2 x6 x10 x14, x3 x7 x11 x15).
+// columns 1..3 after the first round (x1 x5 x9 x13, x2 x6 x10 x14, x3 x7 x11 x15).
 IRS_HD void chacha_prepare(const ChaChaKey& key, uint32_t ctr_hi, uint64_t nonce, uint32_t pre[24]) {
   for (int i = 0; i < 8; i++) pre[i] = key.k[i];
   pre[8] = ctr_hi;
