@@ -265,6 +265,9 @@ class BatchedEngine:
                 dst.append((i, True))
         if len(uniq) > self.max_variants or len(reauth) > self.max_reauth:
             raise ValueError("batch exceeds the engine's variant capacity")
+        for i, _ in reauth:
+            if not 0 <= requests[i].target < self.db_len:
+                raise ValueError(f"reauth target {requests[i].target} of request {i} is not in the DB")
         return uniq, reauth
 
     def _buffers(self):

@@ -171,6 +171,8 @@ def test_submit_rejects_oversized_batches(monkeypatch):
         e.submit([Request(code=z[0], mask=z[1], n_rot=31, mirrored=True) for _ in range(9)])  # 18 variants > 16
     with pytest.raises(ValueError):  # 12 variants fit the count, but need 12 words of rows
         e.submit([Request(code=z[0], mask=z[1], n_rot=31, mirrored=True) for _ in range(6)])
+    with pytest.raises(ValueError):  # reauth target outside the DB
+        e.submit([Request(code=z[0], mask=z[1], n_rot=1, kind="reauth", target=e.db_len)])
     assert e._inflight == [None, None]
     assert not any(isinstance(c, tuple) for c in dm.calls)  # failed before any device work
 
