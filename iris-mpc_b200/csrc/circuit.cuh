@@ -265,6 +265,32 @@ IRS_HD void inject_bit(Comp v, int j, const uint32_t ks[3][16], uint32_t& A0, ui
   A2 = (v2 - 2u * (r02 + z)) & 0xFFFFu;
 }
 
+// Even bits of x to the low half, odd bits to the high half (bit 2k -> k,
+// bit 2k+1 -> 16 + k): the carry bits of elements 2i and 2i+1 then sit at
+// bits i and 16 + i, one 16-bit lane each.
+IRS_HD uint32_t unzip_bits(uint32_t x) {
+  uint32_t t;
+  t = (x ^ (x >> 1)) & 0x22222222u; x ^= t ^ (t << 1);
+  t = (x ^ (x >> 2)) & 0x0C0C0C0Cu; x ^= t ^ (t << 2);
+  t = (x ^ (x >> 4)) & 0x00F000F0u; x ^= t ^ (t << 4);
+  t = (x ^ (x >> 8)) & 0x0000FF00u; x ^= t ^ (t << 8);
+  return x;
+}
+
+// inject_bit for the element pair (2i, 2i+1) in packed 16-bit lanes: V0..V2
+// hold the pair's carry bits (0 or 1 per lane, from unzip_bits), R01 / R12 /
+// R02 the pair's keystream words; returns the parties' packed components.
+IRS_HD void inject_pair(uint32_t V0, uint32_t V1, uint32_t V2, uint32_t R01, uint32_t R12, uint32_t R02,
+                        uint32_t& A0, uint32_t& A1, uint32_t& A2) {
+  const uint32_t X = sub2(V1 ^ V0, R01);  // party 1 -> party 2
+  const uint32_t M2 = V2 * 0xFFFFu;       // lane-wise v2 ? 0xFFFF : 0
+  const uint32_t Y = sub2(R01 & M2, R02); // party 0 -> party 1
+  const uint32_t Z = sub2(M2 & X, R12);   // party 2 -> party 0
+  A0 = sub2(R01, (Y << 1) & 0xFFFEFFFEu);
+  A1 = sub2(X, (R12 << 1) & 0xFFFEFFFEu);
+  A2 = sub2(V2, (add2(R02, Z) << 1) & 0xFFFEFFFEu);
+}
+
 // lift_mpc for one word: the injected correction components of both carries
 // (corr1[p][j], corr2[p][j] = party p's own component, u16) such that
 // mask = sum_p mask_p - (sum_p corr1_p << 16) - (sum_p corr2_p << 17) in Z_2^32.
@@ -321,26 +347,27 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
     // over a small per-thread array: one copy of their code instead of 64
     // unrolled ones keeps the kernel's straight-line code (executed once per
     // word) small enough for the instruction cache.
+    // Elements 2i and 2i+1 share keystream word i of each stream, so the
+    // injection runs on packed 16-bit lanes, a pair per step.
     uint32_t corr[3][16];
-    wr.load(6);
+    {
+      const uint32_t w0 = unzip_bits(c1.c0), w1 = unzip_bits(c1.c1), w2 = unzip_bits(c1.c2);
+      wr.load(6);
 #pragma unroll 1
-    for (int i = 0; i < 16; i++) {
-      uint32_t a[3], b[3];
-      inject_bit(c1, 2 * i, wr.ks, a[0], a[1], a[2]);
-      inject_bit(c1, 2 * i + 1, wr.ks, b[0], b[1], b[2]);
-#pragma unroll
-      for (int p = 0; p < 3; p++) corr[p][i] = a[p] | (b[p] << 16);
+      for (int i = 0; i < 16; i++)
+        inject_pair((w0 >> i) & 0x00010001u, (w1 >> i) & 0x00010001u, (w2 >> i) & 0x00010001u, wr.ks[0][i],
+                    wr.ks[1][i], wr.ks[2][i], corr[0][i], corr[1][i], corr[2][i]);
     }
-    wr.load(7);
+    {
+      const uint32_t w0 = unzip_bits(c2.c0), w1 = unzip_bits(c2.c1), w2 = unzip_bits(c2.c2);
+      wr.load(7);
 #pragma unroll 1
-    for (int i = 0; i < 16; i++) {
-      uint32_t a[3], b[3];
-      inject_bit(c2, 2 * i, wr.ks, a[0], a[1], a[2]);
-      inject_bit(c2, 2 * i + 1, wr.ks, b[0], b[1], b[2]);
+      for (int i = 0; i < 16; i++) {
+        uint32_t a[3];
+        inject_pair((w0 >> i) & 0x00010001u, (w1 >> i) & 0x00010001u, (w2 >> i) & 0x00010001u, wr.ks[0][i],
+                    wr.ks[1][i], wr.ks[2][i], a[0], a[1], a[2]);
 #pragma unroll
-      for (int p = 0; p < 3; p++) {
-        const uint32_t w = corr[p][i];
-        corr[p][i] = ((w + 2u * a[p]) & 0xFFFFu) | (((w >> 16) + 2u * b[p]) << 16);
+        for (int p = 0; p < 3; p++) corr[p][i] = add2(corr[p][i], (a[p] << 1) & 0xFFFEFFFEu);
       }
     }
     // X_p = (mask_p - A1_p<<16 - A2_p<<17) * A - code_p<<16 - [p == 0]
