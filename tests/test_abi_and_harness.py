@@ -38,6 +38,14 @@ def test_library_exports_header_symbols():
     assert exported == set(names)
 
 
+def test_rust_binding_declares_every_header_function():
+    """The Rust `extern` block in INTEGRATION.md declares exactly the
+    functions of include/irisb200.h."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    declared = set(re.findall(r"pub fn (irs_[a-z0-9_]+)\(", text))
+    assert declared == set(header_functions())
+
+
 def test_version_and_errors_without_gpu():
     import irisb200
     lib = irisb200.lib()
