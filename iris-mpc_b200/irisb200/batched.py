@@ -18,6 +18,11 @@ layout into a CUDA graph and replayed; the ChaCha batch id comes from the
 device batch counter, so a replay draws fresh randomness.  The autotuner picks
 the tile width along the query rows and the DB chunk length per padded row
 count by timing the candidates once.
+
+A request and its mirrored variant share one uploaded base share; the row
+descriptor's mirror bit makes the device build the mirrored rotations.
+submit() prepares a batch in page-locked buffers and only enqueues it, so
+two batches can be in flight; collect() returns a batch's results.
 """
 from __future__ import annotations
 
