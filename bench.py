@@ -4,8 +4,9 @@
 Workload (the GPU plain drop-in configuration): 3 parties co-resident on one
 GPU, 64 queries x 31 rotations (1984 query rows in 64 slots of 32) against
 524,288 share-DB entries per party, threshold ratio 0.375 (A = 16384).  One
-step = one batch: the six limb GEMMs (3 parties x code/mask) in one tcgen05
-launch, then the fused threshold + open + rotation OR into the match bitmap.
+step = one batch, the DB scanned in chunks of 65,536 entries (--db-chunk): per
+chunk the six limb GEMMs (3 parties x code/mask) in one tcgen05 launch, then
+the fused threshold + open + rotation OR into the match bitmap.
 One comparison = one (query iris, DB entry) pair over all 31 rotations,
 computed jointly by the three parties.
 
