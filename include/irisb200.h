@@ -65,6 +65,23 @@ int irs_device_manager_synchronize(irs_device_manager* dm);
 /* Device error word: 0, or the code of the first bounded wait that expired. */
 int irs_device_manager_error(irs_device_manager* dm, int* code);
 int irs_device_manager_clear_error(irs_device_manager* dm);
+/* Error codes of the device error word. */
+#define IRS_DEV_ERR_TIMEOUT_FULL 1      /* the GEMM's MMA waited too long for a TMA stage */
+#define IRS_DEV_ERR_TIMEOUT_EMPTY 2     /* the GEMM's loader waited too long for a free stage */
+#define IRS_DEV_ERR_TIMEOUT_ACC_FULL 3  /* the GEMM's epilogue waited too long for its accumulator */
+#define IRS_DEV_ERR_TIMEOUT_ACC_EMPTY 4 /* the GEMM's MMA waited too long for the epilogue */
+#define IRS_DEV_ERR_TIMEOUT_DRAIN 5     /* an exit-time wait for in-flight copies gave up */
+/* Test hook of the failure path (the reference panics on a stuck NCCL or
+ * kernel wait, helpers/device_manager.rs:25-26,330-343, under panic = abort):
+ * the next dot launch of this device manager runs with `wait_limit_ns` as its
+ * bounded-wait limit (1 us .. 10 s; the default is 2 s) and its first CTA
+ * issues no loads, so that CTA's MMA stage wait runs out.  The kernel records
+ * IRS_DEV_ERR_TIMEOUT_FULL in the device error word and returns (no memory
+ * access is skipped or added elsewhere; the other CTAs finish their tiles);
+ * the next synchronising call returns IRS_ERR_DEVICE, the device stays usable,
+ * and irs_device_manager_clear_error resets the word.  One shot; refused
+ * during a graph capture. */
+int irs_device_manager_test_stall_next_dot(irs_device_manager* dm, uint64_t wait_limit_ns);
 /* Device-resident batch counter (the reference advances host-side ChaCha
  * counters instead, ChachaCommon::advance_counter, rng/chacha.rs:32-36):
  * engines and circuits switched to it with
@@ -300,11 +317,13 @@ int irs_circuits_compare_threshold_masked_many(irs_circuits* c, const uint16_t* 
  * irs_circuits_compare_threshold_masked_many, but its scratch lives in a
  * static device array of IRS_NOALLOC_MAX_ELEMENTS / 32 words per party that
  * every GPU loading the library holds until exit; it calls no allocator.
- * n above IRS_NOALLOC_MAX_ELEMENTS is rejected with IRS_ERR_INVALID.  The
- * first call on a device resolves the array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
- * share the array: calls whose work overlaps on the GPU race and must be
- * serialised by the caller. */
+ * n above IRS_NOALLOC_MAX_ELEMENTS is rejected with IRS_ERR_INVALID.  A call
+ * outside stream capture looks up the array's device address
+ * (cudaGetSymbolAddress, so it stays right after a cudaDeviceReset); a call
+ * inside a capture reuses the address of the device's last call outside one,
+ * so make the first call on each device before any stream capture
+ * (IRS_ERR_STATE otherwise).  All calls share the array: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller. */
 #define IRS_NOALLOC_MAX_ELEMENTS (1u << 22)
 int irs_circuits_compare_threshold_masked_many_noalloc(irs_circuits* c, const uint16_t* const code_a[3],
                                                        const uint16_t* const mask_a[3], size_t n,

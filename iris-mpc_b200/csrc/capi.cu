@@ -74,6 +74,7 @@ struct irs_device_manager {
   };
   std::vector<Timer> timers;
   std::map<std::string, std::pair<double, long>> timer_totals;  // label -> (ms, launches)
+  uint64_t stall_limit_ns = 0;  // armed by irs_device_manager_test_stall_next_dot (one shot)
 };
 
 // Brackets one stage launch on stream s with a pair of timing events when the
@@ -328,6 +329,15 @@ int irs_device_manager_error(irs_device_manager* dm, int* code) {
 int irs_device_manager_clear_error(irs_device_manager* dm) {
   CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
   CU(cudaMemset(dm->d_err, 0, sizeof(int)));
+  return IRS_OK;
+}
+
+int irs_device_manager_test_stall_next_dot(irs_device_manager* dm, uint64_t wait_limit_ns) {
+  CHECK(dm, IRS_ERR_INVALID, "dm is NULL");
+  CHECK(wait_limit_ns >= 1000 && wait_limit_ns <= 10000000000ull, IRS_ERR_INVALID,
+        "wait limit %llu ns outside 1 us .. 10 s", (unsigned long long)wait_limit_ns);
+  CHECK(!dm->capturing, IRS_ERR_STATE, "arm the stall outside a graph capture");
+  dm->stall_limit_ns = wait_limit_ns;
   return IRS_OK;
 }
 
@@ -938,6 +948,11 @@ int irs_sharedb_dot_many(irs_sharedb* const* engines, const uint16_t* multiplier
       CU(cudaStreamWaitEvent(s, engines[i]->done, 0));
     }
   if (len) {
+    if (dm->stall_limit_ns && !dm->capturing) {  // one-shot test hook
+      P.test_stall = 1;
+      P.wait_timeout_ns = dm->stall_limit_ns;
+      dm->stall_limit_ns = 0;
+    }
     StageTimer timer(dm, s, "dot");
     CU(launch_limb_gemm(P, engines[0]->block_n, dm->n_sms, s));
   }

@@ -37,7 +37,6 @@ namespace {
 constexpr int kBM = 128;   // DB entries per tile (MMA M)
 constexpr int kBK = 128;   // K bytes per pipeline stage (one 128-byte swizzle row)
 constexpr int kThreads = 320;
-constexpr uint64_t kWaitTimeoutNs = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -67,19 +66,34 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: gives up after kWaitTimeoutNs or when another thread has
+// Bounded wait: gives up after `limit_ns` or when another thread has
 // reported an error, recording `code` in the error word.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t it = 1;; it++) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 255u) == 0) {
       if (has_error(err)) return false;
-      if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+      if (globaltimer_ns() - t0 > limit_ns) {
         set_error(err, code);
         return false;
       }
+    }
+  }
+}
+
+// Exit-time wait for this CTA's own copies or MMAs still in flight: they
+// complete whatever else has failed, so it does not give up on another
+// thread's error -- only after `limit_ns` (recording kErrTimeoutDrain).
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity, int* err, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t it = 1;; it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) {
+      set_error(err, kErrTimeoutDrain);
+      return false;
     }
   }
 }
@@ -217,6 +231,10 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   int* err = P.err;
+  // The MMA's wait for a TMA stage has the launch's limit; every other wait
+  // (which in a failing launch only follows that one) twice as long, so the
+  // first expiry names the stage that never arrived.
+  const uint64_t lim = P.wait_timeout_ns, lim2 = 2 * P.wait_timeout_ns;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::kStages; s++) {
@@ -250,6 +268,9 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
       const bool hinted = P.l2_hint != 0;
       const uint64_t pol_a = (P.l2_hint & 2u) ? policy_evict_first() : policy_evict_normal();
       const uint64_t pol_b = (P.l2_hint & 1u) ? policy_evict_last() : policy_evict_normal();
+      // Test hook (GemmParams::test_stall): CTA 0 issues no loads at all, so
+      // its MMA's first stage wait runs out.  Nothing is in flight to drain.
+      if (P.test_stall && blockIdx.x == 0) ok = false;
       for (int t = blockIdx.x; ok && t < P.total_tiles; t += gridDim.x) {
         Tile tl;
         if (!tile_of(P, t, tl)) break;
@@ -257,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
         const int ya = (int)pr.m0 + tl.m_tile * kBM;
         const int yb = tl.n_tile * BN;
         for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
-          if (!mbar_wait(&empty_bar[stage], phase ^ 1u, err, kErrTimeoutEmpty)) { ok = false; break; }
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1u, err, kErrTimeoutEmpty, lim2)) { ok = false; break; }
           mbar_expect_tx(&full_bar[stage], (uint32_t)C::kStageBytes);
           const int x = (int)ki * kBK;
           if (hinted) {
@@ -278,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
       }
       // Exit: make sure no copy into this CTA's shared memory is still in flight.
       for (int s = 0; s < C::kStages; s++)
-        if (issued[s]) mbar_wait(&full_bar[s], (uint32_t)issued_phase[s], err, kErrTimeoutDrain);
+        if (issued[s]) mbar_wait_drain(&full_bar[s], (uint32_t)issued_phase[s], err, lim2);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
@@ -292,11 +313,11 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
         Tile tl;
         if (!tile_of(P, t, tl)) break;
         const GemmProblem& pr = P.prob[tl.prob];
-        if (!mbar_wait(acc_empty, acc_phase ^ 1u, err, kErrTimeoutAccEmpty)) { ok = false; break; }
+        if (!mbar_wait(acc_empty, acc_phase ^ 1u, err, kErrTimeoutAccEmpty, lim2)) { ok = false; break; }
         acc_phase ^= 1u;
         tc_fence_after();
         for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
-          if (!mbar_wait(&full_bar[stage], phase, err, kErrTimeoutFull)) { ok = false; break; }
+          if (!mbar_wait(&full_bar[stage], phase, err, kErrTimeoutFull, lim)) { ok = false; break; }
           tc_fence_after();
           const uint64_t dal = smem_desc(a_lo + stage * kBM * kBK);
           const uint64_t dah = smem_desc(a_hi + stage * kBM * kBK);
@@ -317,7 +338,7 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
       }
       // Exit: wait until every MMA issued by this thread has completed.
       mma_commit(done_bar);
-      mbar_wait(done_bar, 0, err, kErrTimeoutDrain);
+      mbar_wait_drain(done_bar, 0, err, lim2);
     }
   } else {
     // ---------------- Epilogue (warps 2..9) ----------------
@@ -330,7 +351,7 @@ __global__ void __launch_bounds__(kThreads, 1) limb_gemm_kernel(const __grid_con
       Tile tl;
       if (!tile_of(P, t, tl)) break;
       const GemmProblem& pr = P.prob[tl.prob];
-      if (!mbar_wait(acc_full, acc_phase, err, kErrTimeoutAccFull)) break;
+      if (!mbar_wait(acc_full, acc_phase, err, kErrTimeoutAccFull, lim2)) break;
       acc_phase ^= 1u;
       tc_fence_after();
       uint32_t packed[kCols / 2];
@@ -505,6 +526,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   const int cluster = blockIdx.x >> 1;
   const int n_clusters = gridDim.x >> 1;
   int* err = P.err;
+  const uint64_t lim = P.wait_timeout_ns, lim2 = 2 * P.wait_timeout_ns;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::kStages; s++) {
@@ -543,7 +565,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         const int ya = (int)pr.m0 + tl.m_tile * kBM2 + (int)rank * 128;
         const int yb = tl.n_tile * BN + (int)rank * C::kHalfN;
         for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
-          if (!mbar_wait(&empty_bar[stage], phase ^ 1u, err, kErrTimeoutEmpty)) { ok = false; break; }
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1u, err, kErrTimeoutEmpty, lim2)) { ok = false; break; }
           if (leader) mbar_expect_tx(&full_bar[stage], (uint32_t)(2 * C::kStageBytes));
           const uint32_t fb = map_to_rank(&full_bar[stage], 0);
           const int x = (int)ki * kBK;
@@ -560,7 +582,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       // of that stage have landed.
       if (leader)
         for (int s = 0; s < C::kStages; s++)
-          if (issued[s]) mbar_wait(&full_bar[s], (uint32_t)issued_phase[s], err, kErrTimeoutDrain);
+          if (issued[s]) mbar_wait_drain(&full_bar[s], (uint32_t)issued_phase[s], err, lim2);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer (leader CTA only) ----------------
@@ -574,11 +596,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         Tile tl;
         if (!tile_of2(P, t, tl)) break;
         const GemmProblem& pr = P.prob[tl.prob];
-        if (!mbar_wait(acc_empty, acc_phase ^ 1u, err, kErrTimeoutAccEmpty)) { ok = false; break; }
+        if (!mbar_wait(acc_empty, acc_phase ^ 1u, err, kErrTimeoutAccEmpty, lim2)) { ok = false; break; }
         acc_phase ^= 1u;
         tc_fence_after();
         for (uint32_t ki = 0; ki < pr.k_iters; ki++) {
-          if (!mbar_wait(&full_bar[stage], phase, err, kErrTimeoutFull)) { ok = false; break; }
+          if (!mbar_wait(&full_bar[stage], phase, err, kErrTimeoutFull, lim)) { ok = false; break; }
           tc_fence_after();
           const uint64_t dal = smem_desc(a_lo + stage * 128 * kBK);
           const uint64_t dah = smem_desc(a_hi + stage * 128 * kBK);
@@ -600,7 +622,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(done_bar))
                    : "memory");
-      mbar_wait(done_bar, 0, err, kErrTimeoutDrain);
+      mbar_wait_drain(done_bar, 0, err, lim2);
     }
   } else {
     // ---------------- Epilogue (warps 2..9, both CTAs) ----------------
@@ -614,7 +636,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       Tile tl;
       if (!tile_of2(P, t, tl)) break;
       const GemmProblem& pr = P.prob[tl.prob];
-      if (!mbar_wait(acc_full, acc_phase, err, kErrTimeoutAccFull)) break;
+      if (!mbar_wait(acc_full, acc_phase, err, kErrTimeoutAccFull, lim2)) break;
       acc_phase ^= 1u;
       tc_fence_after();
       uint32_t packed[kCols / 2];
@@ -778,7 +800,8 @@ static uint32_t gemm_l2_hint() {
 }
 
 cudaError_t launch_limb_gemm(GemmParams& P, int block_n, int n_sms, cudaStream_t stream) {
-  const bool pair = gemm_use_pair(block_n);
+  const bool pair = gemm_use_pair(block_n) && !P.test_stall;  // the stall hook is the one-SM kernel's
+  if (P.wait_timeout_ns == 0) P.wait_timeout_ns = kGemmWaitTimeoutNs;
   P.l2_hint = gemm_l2_hint();
   const uint32_t bm = pair ? (uint32_t)kBM2 : (uint32_t)kBM;
   P.total_tiles = 0;

@@ -31,6 +31,7 @@ struct alignas(64) GemmProblem {
 };
 
 constexpr int kMaxGemmProblems = 6;
+constexpr uint64_t kGemmWaitTimeoutNs = 2000000000ull;  // default limit of a bounded wait: 2 s
 
 struct GemmParams {
   GemmProblem prob[kMaxGemmProblems];
@@ -40,6 +41,12 @@ struct GemmParams {
   // L2 eviction priority of the TMA loads: bit 0 = query planes evict_last
   // (re-read by every DB tile), bit 1 = DB planes evict_first (streamed).
   uint32_t l2_hint;
+  // Limit of the MMA's wait for a TMA stage; the other waits get twice this.
+  // 0 = kGemmWaitTimeoutNs.
+  uint64_t wait_timeout_ns;
+  // Test hook: CTA 0 issues no TMA loads, so its MMA's first stage wait runs
+  // out (kErrTimeoutFull) and the kernel returns with the error word set.
+  uint32_t test_stall;
 };
 
 // Builds a 2-D u8 tensor map (inner dim K, outer dim rows) with 128x`box_rows`

@@ -32,27 +32,37 @@ constexpr size_t kNoallocWords = kNoallocMaxElements / 32;
 // Per-word result components of the three parties: [3][kNoallocWords].
 static __device__ __align__(256) uint32_t g_noalloc_comp[3 * kNoallocWords];
 
-// Device addresses of g_noalloc_comp, resolved once per device.
+// Device addresses of g_noalloc_comp, per device.  A call made outside stream
+// capture looks the address up afresh (cudaGetSymbolAddress is a table lookup,
+// and a fresh lookup stays right after cudaDeviceReset has reloaded the
+// module); a call inside a capture uses the address cached by the last call
+// outside one, so the first call on a device must come before any capture.
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 uint32_t* g_comp_ptr[kMaxDevices] = {};
 
-int comp_ptr_for(int device, uint32_t** out) {
-  if (device < 0 || device >= kMaxDevices) return IRS_ERR_INVALID;
+// `device` is the current device.  Returns IRS_OK or an error status with the
+// thread's last-error message set.
+int comp_ptr_for(int device, bool capturing, uint32_t** out) {
+  if (device < 0 || device >= kMaxDevices)
+    return set_error(IRS_ERR_INVALID, "device ordinal %d is outside the %d devices the no-allocation entry point "
+                     "supports", device, kMaxDevices);
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_comp_ptr[device]) {
-    int cur = -1;
-    if (cudaGetDevice(&cur) != cudaSuccess) return IRS_ERR_CUDA;
-    if (cur != device && cudaSetDevice(device) != cudaSuccess) return IRS_ERR_CUDA;
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_comp);
-    if (cur != device) cudaSetDevice(cur);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return IRS_ERR_CUDA;
-    }
-    g_comp_ptr[device] = static_cast<uint32_t*>(p);
+  if (capturing) {
+    if (!g_comp_ptr[device])
+      return set_error(IRS_ERR_STATE, "the first no-allocation call on device %d must come before any stream "
+                       "capture (it resolves the scratch array's device address)", device);
+    *out = g_comp_ptr[device];
+    return IRS_OK;
   }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_comp);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return set_error(IRS_ERR_CUDA, "cudaGetSymbolAddress of the no-allocation scratch failed on device %d: %s",
+                     device, cudaGetErrorString(e));
+  }
+  g_comp_ptr[device] = static_cast<uint32_t*>(p);
   *out = g_comp_ptr[device];
   return IRS_OK;
 }
@@ -97,11 +107,16 @@ extern "C" int irs_circuits_compare_threshold_masked_many_noalloc(irs_circuits* 
       return set_error(IRS_ERR_INVALID, "share pointers must be 16-byte aligned");
   }
   if (cudaSetDevice(v.device) != cudaSuccess) return set_error(IRS_ERR_CUDA, "cudaSetDevice(%d) failed", v.device);
-  uint32_t* comp = nullptr;
-  rc = comp_ptr_for(v.device, &comp);
-  if (rc) return set_error(rc, "cudaGetSymbolAddress of the no-allocation scratch failed on device %d", v.device);
-  if (n == 0) return IRS_OK;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : v.stream0;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(IRS_ERR_CUDA, "cudaStreamIsCapturing failed");
+  }
+  uint32_t* comp = nullptr;
+  rc = comp_ptr_for(v.device, cap != cudaStreamCaptureStatusNone, &comp);
+  if (rc) return rc;
+  if (n == 0) return IRS_OK;
   ThresholdParams P = {};
   for (int p = 0; p < 3; p++) {
     P.key[p] = v.keys[p];

@@ -28,6 +28,13 @@ THRESHOLD_ANON_STATS_A = 16384  # ratio 0.375 (iris-mpc-gpu/src/dot/mod.rs:14)
 
 IRS_OK = 0
 IRS_ERR_OVERFLOW = -6
+IRS_ERR_DEVICE = -5
+# device error word codes (include/irisb200.h IRS_DEV_ERR_*)
+DEV_ERR_TIMEOUT_FULL = 1
+DEV_ERR_TIMEOUT_EMPTY = 2
+DEV_ERR_TIMEOUT_ACC_FULL = 3
+DEV_ERR_TIMEOUT_ACC_EMPTY = 4
+DEV_ERR_TIMEOUT_DRAIN = 5
 
 
 class IrisError(RuntimeError):
@@ -56,6 +63,7 @@ _SIGS = {
     "irs_device_manager_synchronize": [_vp],
     "irs_device_manager_error": [_vp, C.POINTER(_i)],
     "irs_device_manager_clear_error": [_vp],
+    "irs_device_manager_test_stall_next_dot": [_vp, _u64],
     "irs_device_manager_sm_count": [_vp, C.POINTER(_i)],
     "irs_device_manager_mem_info": [_vp, C.POINTER(_sz), C.POINTER(_sz)],
     "irs_device_manager_set_host_sync": [_vp, _i],
@@ -392,6 +400,15 @@ class DeviceManager:
         c = C.c_int()
         _check(lib().irs_device_manager_error(self.h, C.byref(c)))
         return c.value
+
+    def clear_error(self) -> None:
+        _check(lib().irs_device_manager_clear_error(self.h))
+
+    def test_stall_next_dot(self, wait_limit_ns: int) -> None:
+        """Test hook: the next dot launch runs with this bounded-wait limit and
+        its first CTA loads nothing, so that CTA's stage wait runs out and the
+        kernel records DEV_ERR_TIMEOUT_FULL (irs_device_manager_test_stall_next_dot)."""
+        _check(lib().irs_device_manager_test_stall_next_dot(self.h, int(wait_limit_ns)))
 
     def set_batch_counter(self, batch_id: int, stream=None) -> None:
         _check(lib().irs_device_manager_set_batch_counter(self.h, batch_id, stream))

@@ -63,21 +63,29 @@ def merge_final_results(per_rank_final) -> np.ndarray:
 def merge_match_lists(per_rank_counts, per_rank_ids, cap: int | None = None):
     """Union of the shards' match lists, as sorted global indices per query.
     per_rank_ids[r][q] holds the first min(count, width) local matches of
-    query q on shard r.  Returns (total counts, [sorted global ids per query])
-    with at most `cap` ids kept per query when cap is given."""
+    query q on shard r (width = the list's length).  Returns (total counts,
+    [sorted global ids per query]).
+
+    Each list keeps at most min(cap, width) ids (width alone when cap is
+    None): a shard's ids beyond its width are unknown, so only the smallest
+    `width` merged ids are certain to be the smallest global matches (every
+    one of them is among its own shard's smallest `width`).  A query whose
+    total count exceeds its list's length was truncated."""
     world = len(per_rank_counts)
     nq = len(per_rank_counts[0])
     counts = np.zeros(nq, np.int64)
     lists = []
     for q in range(nq):
         ids = []
+        width = min(len(per_rank_ids[r][q]) for r in range(world))
         for r in range(world):
             n = int(per_rank_counts[r][q])
             counts[q] += n
             local = np.asarray(per_rank_ids[r][q][: min(n, len(per_rank_ids[r][q]))], np.int64)
             ids.append(local * world + r)
         merged = np.sort(np.concatenate(ids)) if ids else np.zeros(0, np.int64)
-        lists.append(merged[:cap] if cap is not None else merged)
+        keep = width if cap is None else min(cap, width)
+        lists.append(merged[:keep])
     return counts, lists
 
 

@@ -64,13 +64,19 @@ def build(force: bool = False) -> None:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def build_ref() -> bool:
-    """Compile the reference's ChaCha12 kernel into _ref/ when the reference
-    tree is present (this machine); on a machine without it the prebuilt
-    cubin, if any, is used as is.  Returns whether the cubin exists."""
-    ref = os.environ.get("IRIS_REFERENCE", "/root/reference")
-    if os.path.isdir(ref):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True)
+def build_ref(ref_root: str | None = None) -> bool:
+    """Compile the reference's ChaCha12 and Phase-1 kernels into _ref/ from a
+    worldcoin/iris-mpc checkout at `ref_root` (default: the IRIS_REFERENCE
+    environment variable).  One of the two is required: without a checkout
+    there is nothing to compile, and the prebuilt cubins, if any, are used as
+    they are.  Returns whether both cubins exist."""
+    ref = ref_root or os.environ.get("IRIS_REFERENCE")
+    if not ref:
+        raise ValueError("build_ref needs the path of a worldcoin/iris-mpc checkout: pass ref_root or set "
+                         "IRIS_REFERENCE")
+    if not os.path.isdir(ref):
+        raise ValueError(f"build_ref: {ref} is not a directory (expected a worldcoin/iris-mpc checkout)")
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True)
     return os.path.exists(REF_CHACHA_CUBIN) and os.path.exists(REF_DOT_CUBIN)
 
 

@@ -48,4 +48,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IRIS_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <path to a worldcoin/iris-mpc checkout> (or set IRIS_REFERENCE)")
+    main(root)

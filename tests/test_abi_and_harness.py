@@ -39,9 +39,9 @@ def test_library_exports_header_symbols():
 
 
 def test_rust_binding_declares_every_header_function():
-    """The Rust `extern` block in INTEGRATION.md declares exactly the
+    """The Rust `extern` block of include/irisb200.rs declares exactly the
     functions of include/irisb200.h."""
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    text = open(os.path.join(ROOT, "include", "irisb200.rs")).read()
     declared = set(re.findall(r"pub fn (irs_[a-z0-9_]+)\(", text))
     assert declared == set(header_functions())
 

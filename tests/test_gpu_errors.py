@@ -162,3 +162,42 @@ def test_stage_timers(dm):
         c.close()
         for e in ce + me:
             e.close()
+
+
+def test_expired_bounded_wait_reports_and_device_recovers(dm, oracle):
+    """The GEMM's bounded waits end in an error status, not a hang: with the
+    test hook armed, the first CTA of the next dot issues no loads, so its MMA's
+    stage wait runs out after 1 ms.  The kernel records
+    DEV_ERR_TIMEOUT_FULL and returns; the next synchronising call fails with
+    IRS_ERR_DEVICE (the reference panics on a stuck wait instead,
+    iris-mpc-gpu/src/helpers/device_manager.rs:25-26,330-343); after
+    clear_error the same engine's next dot equals the oracle."""
+    rng = np.random.default_rng(11)
+    n, q_len = 1024, 32
+    db = rng.integers(0, 65535, (n, 12800)).astype(np.uint16)
+    q = rng.integers(0, 65535, (q_len, 12800)).astype(np.uint16)
+    e = irisb200.ShareDB(0, dm, n, q_len, 12800, W.SEEDS[0], is_remote=False)
+    try:
+        e.alloc_db(n)
+        e.load_records(0, db)
+        e.query_upload(q)
+        dm.synchronize()
+        assert dm.error_code() == 0
+        dm.test_stall_next_dot(1_000_000)
+        e.dot(0, n, 1)  # the launch itself succeeds
+        with pytest.raises(irisb200.IrisError) as ei:
+            dm.synchronize()
+        assert ei.value.code == irisb200.IRS_ERR_DEVICE, str(ei.value)
+        assert dm.error_code() == irisb200.DEV_ERR_TIMEOUT_FULL
+        dm.clear_error()
+        assert dm.error_code() == 0
+        # the hook is one-shot: the next dot runs normally and is exact
+        e.dot(0, n, 1)
+        got = e.fetch_results(n)
+        assert np.array_equal(got, oracle.dot_u16(q, db))
+        dm.synchronize()
+        # out-of-range limits are refused on the host
+        _raises(lambda: dm.test_stall_next_dot(0), -1)
+    finally:
+        dm.clear_error()
+        e.close()

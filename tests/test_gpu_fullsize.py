@@ -1,12 +1,17 @@
 """Parity at the benchmark's full size: 64 queries x 31 rotations against
 524,288 share-DB entries per party (3 parties, 60 GB resident).  The whole DB
 is scanned in one chunk and again in four chunks; the bitmaps must be equal
-(chunking invariance), every planted near-duplicate must be found, blocks
-of entries at the start, the end and around the planted entries must equal
-the CPU path on the same shares (records read back from the device), and the
-batched engine (packed rows, captured graph) and the continuous server
-(chunked circular scan, requests admitted mid-scan) must return the same
-matches."""
+(chunking invariance), every planted near-duplicate must be found, and the
+CPU path on the same shares (records read back from the device) must agree
+on blocks of entries at the start, the end and around the planted entries
+and on a strided sample of 4,096 entries spread over the whole DB (one entry
+in every 128, at varying positions within the warp's 32).  The batched engine
+(packed rows, captured graph) and the continuous server (chunked circular
+scan, requests admitted mid-scan) must return the same matches, and a mixed
+batch (1/16/31 centred rotations, mirrored orientations, reauth requests)
+must agree with the CPU path on the strided sample, the planted entries and
+the reauth targets (the predicate of iris-mpc-gpu/tests/threshold.rs:110-124,
+ORed over each variant's rotations)."""
 from __future__ import annotations
 
 import numpy as np
@@ -54,8 +59,15 @@ def test_full_size_parity(dm, oracle):
             ms = np.stack([me[p].fetch_records(first, n) for p in range(3)])
             exp = W.expected_bitmap(oracle, qc, qm, cs, ms, A)
             assert np.array_equal(got[:, first:first + n], exp), f"entries {first}..{first + n}"
+        # strided sample over the whole DB, planted entries included
+        sample = sorted(set([128 * k + (37 * k) % 128 for k in range(M // 128)] +
+                            [e for e, _ in planted.values()]))
+        s_cs = np.stack([np.concatenate([ce[p].fetch_records(e, 1) for e in sample]) for p in range(3)])
+        s_ms = np.stack([np.concatenate([me[p].fetch_records(e, 1) for e in sample]) for p in range(3)])
+        exp = W.expected_bitmap(oracle, qc, qm, s_cs, s_ms, A)
+        assert np.array_equal(got[:, sample], exp), "strided sample differs from the CPU path"
         # the batched engine on the same queries (all 31 rotations) gives the same rows
-        from irisb200.batched import BatchedEngine, Request
+        from irisb200.batched import BatchedEngine, Request, centred_rotations
         eng = BatchedEngine(dm, ce, me, c, max_variants=NQ, max_reauth=16, threshold_a=A, autotune=False)
         try:
             res = eng.run([Request(code=qc[:, j], mask=qm[:, j]) for j in range(NQ)])
@@ -63,6 +75,38 @@ def test_full_size_parity(dm, oracle):
             eng.close()
         for j in range(NQ):
             assert res[j].matches == np.nonzero(got[j])[0].tolist()[:256], f"batched query {j}"
+        # a mixed batch against the CPU path: uneven rotations, mirrors, reauth
+        reqs = []
+        for j in range(NQ):
+            kind = "reauth" if j % 5 == 4 else "uniqueness"
+            target = -1
+            if kind == "reauth":
+                target = planted[j][0] if j in planted else sample[(j * 611) % len(sample)]
+            reqs.append(Request(code=qc[:, j], mask=qm[:, j], n_rot=(1, 16, 31)[j % 3], mirrored=j % 2 == 1,
+                                kind=kind, target=target))
+        eng = BatchedEngine(dm, ce, me, c, max_variants=2 * NQ, max_reauth=32, threshold_a=A, autotune=False)
+        try:
+            mres = eng.run(reqs)
+        finally:
+            eng.close()
+        pos = {e: i for i, e in enumerate(sample)}
+        for j, r in enumerate(reqs):
+            rot = list(centred_rotations(r.n_rot))
+            for mir in ([False, True] if r.mirrored else [False]):
+                if r.kind == "reauth":
+                    t_cs = np.stack([ce[p].fetch_records(r.target, 1) for p in range(3)])
+                    t_ms = np.stack([me[p].fetch_records(r.target, 1) for p in range(3)])
+                    hit = bool(W.expected_variant_hits(oracle, t_cs, t_ms, qc[:, j], qm[:, j], rot, mir, [0], A))
+                    got_hit = mres[j].reauth_mirror_match if mir else mres[j].reauth_match
+                    assert got_hit == hit, f"reauth request {j} (mirrored={mir}) against {r.target}"
+                    continue
+                exp_hits = W.expected_variant_hits(oracle, s_cs, s_ms, qc[:, j], qm[:, j], rot, mir,
+                                                   np.arange(len(sample)), A)
+                ids = mres[j].mirror_matches if mir else mres[j].matches
+                cut = ids[-1] if len(ids) == 256 else M  # a full list covers the entries up to its last id
+                got_s = sorted(e for e in ids if e in pos)
+                exp_s = sorted(sample[i] for i in exp_hits if sample[i] <= cut)
+                assert got_s == exp_s, f"batched request {j} (n_rot={r.n_rot}, mirrored={mir}) on the sample"
         # and the continuous server (eight 65,536-entry steps per request, staggered arrivals)
         from irisb200.serving import ContinuousServer
         srv = ContinuousServer(dm, ce, me, c, chunk=65536, row_capacity=NQ * 32, max_variants=NQ, max_reauth=4,
