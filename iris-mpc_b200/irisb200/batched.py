@@ -63,6 +63,8 @@ class Result:
     mirror_matches: list = field(default_factory=list)  # matched entries of the mirrored variant
     reauth_match: bool | None = None
     reauth_mirror_match: bool | None = None
+    match_count: int | None = None         # untruncated number of matches (lists keep the lowest 256)
+    mirror_match_count: int | None = None
 
 
 @dataclass
@@ -418,8 +420,10 @@ class BatchedEngine:
             ids = sorted(matches[v, :min(int(counters[v]), MAX_MATCHES_LEN)].tolist())
             if mir:
                 results[i].mirror_matches = ids
+                results[i].mirror_match_count = int(counters[v])
             else:
                 results[i].matches = ids
+                results[i].match_count = int(counters[v])
         bits = buf["rbits"]
         for v, (i, mir) in enumerate(ticket.reauth):
             hit = bool((int(bits[v, v // 32]) >> (v % 32)) & 1)  # variant v against subset record v

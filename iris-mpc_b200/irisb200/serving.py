@@ -429,8 +429,10 @@ class ContinuousServer:
                     hits = ids[i, : min(int(counts[i]), MAX_MATCHES_LEN)].tolist()
                     if v.mirrored:
                         res.mirror_matches = hits
+                        res.mirror_match_count = int(counts[i])
                     else:
                         res.matches = hits
+                        res.match_count = int(counts[i])
                 out.append(Completion(f.idx, f.arrival, now, res))
             return out
         return handler
@@ -630,8 +632,10 @@ class PlainBatchServer:
                 hits = ids[v, : min(int(counts[v]), ids.shape[1])].tolist()
                 if mir:
                     out[j].mirror_matches = hits
+                    out[j].mirror_match_count = int(counts[v])
                 else:
                     out[j].matches = hits
+                    out[j].match_count = int(counts[v])
         self.batches += 1
         return [Completion(items[j][0], items[j][1], now, out[j]) for j in range(len(items))]
 
