@@ -16,6 +16,16 @@ computed jointly by the three parties.
            device-side rotation expansion, GEMMs, threshold, result merge and
            D2H of the per-query results.
 
+Further legs of the default run, on the same engines and DB (rank 0 of a
+1-GPU run): `latency` (200 plain batches after 20 warm-up, each bracketed by
+CUDA events), `batched` (100 batches of 256 uneven requests through
+BatchedEngine), `serving` (ContinuousServer at 300 / 600 / 1000 requests/s,
+5 s of Poisson arrivals each), the cuBLAS limb GEMMs of the reference on the
+same shapes, and `sweep` (the GEMM and comparison roofline sweep, each row
+timed for at least a second with its own clock record).  `roofline` is the
+limb GEMM's, `roofline_threshold` the threshold kernel's (instruction issue),
+`cycles_per_batch` the GEMM's and cuBLAS's device time x sampled SM clock.
+
 The DB (60.4 GB for the three parties) is far larger than L2, so no L2 flush
 is needed between steps.  Synthetic seeded data (no dataset exists for this
 workload).  `--impl reference` times the CPU restatement of the reference's
@@ -72,8 +82,19 @@ def parse():
     ap.add_argument("--db-chunk", type=int, default=65536,
                     help="plain step: DB entries per GEMM + threshold launch pair (0 = whole DB per launch)")
     ap.add_argument("--serving-arms", default="served,plain", help="serving: which servers to run")
-    ap.add_argument("--serving-rate", type=float, default=600.0,
-                    help="default run: offered load of its serving leg, requests/s (0 = skip)")
+    ap.add_argument("--serving-rates-leg", default="300,600,1000",
+                    help="default run: offered loads of its serving leg, requests/s (empty = skip)")
+    ap.add_argument("--serving-leg-seconds", type=float, default=5.0,
+                    help="default run: seconds of Poisson arrivals per offered load of the serving leg")
+    ap.add_argument("--latency-batches", type=int, default=200,
+                    help="default run: plain batches timed one by one for the latency percentiles (0 = skip)")
+    ap.add_argument("--latency-warmup", type=int, default=20, help="default run: warm-up batches before them")
+    ap.add_argument("--batched-batches", type=int, default=100,
+                    help="default run: batched-leg batches timed one at a time")
+    ap.add_argument("--no-sweep", action="store_true", help="default run: skip the roofline sweep leg")
+    ap.add_argument("--no-fused", action="store_true", help="default run: skip the fused-scan leg")
+    ap.add_argument("--sweep-seconds", type=float, default=1.0,
+                    help="sweep: minimum timed seconds per row (each row carries its own clock record)")
     return ap.parse_args()
 
 
@@ -197,6 +218,18 @@ def cpu_baseline(n_query=8, n_db=8192, min_seconds=10.0):
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{n_query} queries x 31 rotations vs {n_db} entries, 3 parties, {reps} pass(es), "
                       f"{el:.1f} s, OpenMP on {cores} threads"}
+
+
+def pct(values, q: float) -> float:
+    """Nearest-rank percentile q (0..100) of a non-empty sample."""
+    v = sorted(values)
+    k = max(0, min(len(v) - 1, -(-int(round(q * len(v))) // 100) - 1))
+    return v[k]
+
+
+def lat_summary(ms) -> dict:
+    return {"n": len(ms), "p50": pct(ms, 50), "p90": pct(ms, 90), "p99": pct(ms, 99), "mean": statistics.mean(ms),
+            "max": max(ms)}
 
 
 def measure_int8_peak(torch, n=16384):
@@ -410,6 +443,7 @@ def run_ours(args):
         end.record(s0)
         end.synchronize()
     dm.synchronize()
+    clk_value = clk.summary(clk.windows[-1])
     total_ms = begin.elapsed_time(end)
     gemm_ms = [sum(e[0].elapsed_time(e[1]) for e in evs[i]) for i in range(args.steps)]  # per step, all chunks
     thr_ms = [sum(e[1].elapsed_time(e[2]) for e in evs[i]) for i in range(args.steps)]
@@ -426,6 +460,67 @@ def run_ours(args):
     dc.join_db_matches(NQ, M)
     final, counters, _ = dc.fetch_final_results(NQ)
     planted_found = sum(1 for j, (e, _) in planted.items() if final[j] <= e and counters[j] >= 1)
+
+    # ---------------- fused-scan leg: the same batch, GEMM + threshold in one kernel per chunk ----------------
+    fused = None
+    if not args.no_fused and n_rows % 128 == 0:
+        dcf = irisb200.DistanceComparator(dm, NQ, M, match_list_cap=1 << 16)
+
+        def fused_step():
+            dcf.reset()
+            for off, ln in chunks:
+                dcf.scan_fused(c, ce, me, off, ln, A, n_slots=NQ)
+        for _ in range(args.warmup):
+            fused_step()
+        dm.synchronize()
+        fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with clk.mark():
+            fa.record(s0)
+            for _ in range(args.steps):
+                fused_step()
+            fb.record(s0)
+            fb.synchronize()
+        f_ms = fa.elapsed_time(fb) / args.steps
+        f_clk = clk.summary(clk.windows[-1])
+        # the fused pass must give the two-launch pass's results on the same batch
+        dcf.join_db_matches(NQ, M)
+        ff = dcf.fetch_final_results(NQ)
+        dc.reset()
+        scan()
+        dc.join_db_matches(NQ, M)
+        fs = dc.fetch_final_results(NQ)
+        same = all(np.array_equal(a, b) for a, b in zip(ff, fs))
+        dcf.close()
+        fused = {"value": comps / (f_ms * 1e-3), "unit": UNIT, "ms_per_batch": f_ms, "vs_value": per_step / f_ms,
+                 "results_equal_two_launch_path": bool(same), "clocks": f_clk,
+                 "kernel": f"fused_scan_kernel (six limb GEMMs + threshold/open/OR, 128x128 tiles, one launch per "
+                           f"{chunks[0][1]}-entry chunk, {len(chunks)} per batch)",
+                 "timing": "CUDA events around the timed steps on the launching stream, as for value"}
+        if f_clk.get("sm_mhz"):
+            fused["cycles_per_batch"] = f_ms * 1e-3 * f_clk["sm_mhz"] * 1e6
+
+    # ---------------- latency leg: batches back to back, each bracketed by CUDA events ----------------
+    latency = None
+    if args.latency_batches > 0:
+        for _ in range(args.latency_warmup):
+            device_step()
+        dm.synchronize()
+        lev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.latency_batches)]
+        with clk.mark():
+            for a, b in lev:
+                a.record(s0)
+                device_step()
+                b.record(s0)
+            lev[-1][1].synchronize()
+        lat_b = [a.elapsed_time(b) for a, b in lev]
+        latency = lat_summary(lat_b)
+        latency.update(warmup=args.latency_warmup, clocks=clk.summary(clk.windows[-1]),
+                       comparisons_per_s=comps * len(lat_b) / (sum(lat_b) * 1e-3),
+                       rows_x_entries_per_s=NQ * 31 * M * len(lat_b) / (sum(lat_b) * 1e-3),
+                       timing="device time of each plain batch (comparator reset, 8 chunk pairs of GEMM + "
+                              "threshold/open/OR), CUDA events on the launching stream, batches back to back "
+                              "after the warm-up; queries resident")
 
     # ---------------- end-to-end timing through the public API ----------------
     h2d = 3 * NQ * (K_CODE + K_MASK) * 2
@@ -455,6 +550,7 @@ def run_ours(args):
             e2e_step()
             lat.append((time.perf_counter() - ts) * 1e3)
         e2e_s = time.perf_counter() - t0
+    clk_e2e = clk.summary(clk.windows[-1])
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -473,9 +569,10 @@ def run_ours(args):
             eng.run(reqs)
         dm.synchronize()
         blat = []
+        n_bb = max(args.steps, args.batched_batches)
         with clk.mark():
             tb = time.perf_counter()
-            for _ in range(args.steps):  # one batch at a time
+            for _ in range(n_bb):  # one batch at a time
                 ts = time.perf_counter()
                 bres = eng.run(reqs)
                 blat.append((time.perf_counter() - ts) * 1e3)
@@ -507,11 +604,13 @@ def run_ours(args):
                              if reqs[j].kind == "uniqueness" and 15 - r in centred_rotations(reqs[j].n_rot))
         eng.close()
         batched = {
-            "value": bcomp * args.steps / tb, "unit": UNIT,
-            "vs_plain_e2e": (bcomp * args.steps / tb) / e2e_value,
-            "latency_ms": {"p50": sorted(blat)[len(blat) // 2], "p99": max(blat)},
-            "pipelined": {"value": bcomp * args.steps / tp, "unit": UNIT,
-                          "latency_ms": {"p50": sorted(plat)[len(plat) // 2], "p99": max(plat)},
+            "value": bcomp * n_bb / tb, "unit": UNIT, "batches": n_bb,
+            "vs_plain_e2e": (bcomp * n_bb / tb) / e2e_value,
+            "rows_x_entries_per_s": (rows * M + sum(r.n_rot * (2 if r.mirrored else 1) for r in reqs
+                                                    if r.kind == "reauth")) * n_bb / tb,
+            "latency_ms": lat_summary(blat),
+            "pipelined": {"value": bcomp * args.steps / tp, "unit": UNIT, "batches": args.steps,
+                          "latency_ms": lat_summary(plat),
                           "what": "the same batches with two in flight (BatchedEngine.submit / collect: the "
                                   "host prepares batch k+1 while the GPU runs batch k); latency = submit to "
                                   "collect, including the wait for the batch ahead"},
@@ -531,7 +630,8 @@ def run_ours(args):
 
     # ---------------- serving leg: continuous batching under Poisson arrivals ----------------
     serving = None
-    if reqs and args.serving_rate > 0:
+    rates = [float(x) for x in args.serving_rates_leg.split(",") if x]
+    if reqs and rates:
         from irisb200.serving import ContinuousServer
         nq_s = 512
         spl = {j: (int((j * 7919 + 13) % M), (j * 7) % 31 - 15) for j in range(0, nq_s, 10)}
@@ -541,17 +641,40 @@ def run_ours(args):
                                max_reauth=64, threshold_a=A, seeds=seeds, db_capacity=M + 256)
         warm = request_mix(40, sqc, sqm, spl, M, seed=99)
         srv.serve([0.0] * len(warm), warm)
-        serving = serve_load(srv, srv, args.serving_rate, 2.0, 0, (sqc, sqm, spl, M, app_c, app_m), clk)
-        serving["vs_plain_value"] = serving["comparisons_per_s"] / value
-        serving["config"] = {"workload": "continuous serving: Poisson arrivals, 80% uniqueness / 20% reauth, 1% "
-                                         "appends, rotations 1/16/31, 50% mirrored, 2 s of arrivals",
-                             "row_capacity": q_cap, "chunk": 65536}
+        loads = []
+        for li, lam in enumerate(rates):
+            st = serve_load(srv, srv, lam, args.serving_leg_seconds, li, (sqc, sqm, spl, M, app_c, app_m), clk)
+            st["vs_plain_value"] = st["comparisons_per_s"] / value
+            st["rows_x_entries_per_s"] = (st["mean_used_rows_per_step"] * 65536 /
+                                          (st["mean_step_interval_ms"] * 1e-3))
+            loads.append(st)
+        under = [x for x in loads if x["p99_ms"] < 1000.0]
+        over = [x for x in loads if x["p99_ms"] >= 1000.0]
+        serving = {
+            "loads": loads,
+            "saturation_requests_per_s": max(x["requests_per_s"] for x in loads),
+            "p99_below_1s_up_to_offered": max((x["offered_requests_per_s"] for x in under), default=None),
+            "p99_above_1s_from_offered": min((x["offered_requests_per_s"] for x in over), default=None),
+            "config": {"workload": "continuous serving: Poisson arrivals, 80% uniqueness / 20% reauth, 1% appends, "
+                                   f"rotations 1/16/31, 50% mirrored, {args.serving_leg_seconds:g} s of arrivals per "
+                                   "offered load",
+                       "row_capacity": q_cap, "chunk": 65536,
+                       "saturation": "the highest completed requests/s over the offered loads (a request counts "
+                                     "from its arrival to its completion; the rate runs to the last completion)"},
+        }
         srv.close()
         for e in ce + me:
             e.set_db_len(M)
     cublas_ms = cublas_clk = None
     if rank == 0 and not args.no_cublas:
         cublas_ms, cublas_clk = cublas_limb_gemms(torch, M, NQ * 31, clk=clk)
+    peak = measure_int8_peak(torch) if rank == 0 else None
+    # the 3-party DB is freed before the sweep's single-party DBs are built
+    for o in ce + me + [c, dc]:
+        o.close()
+    sweep = None
+    if rank == 0 and world == 1 and not args.no_sweep:
+        sweep = sweep_leg(dm, clk, args.sweep_seconds)
     clk.__exit__(None, None, None)
 
     result = None
@@ -560,7 +683,6 @@ def run_ours(args):
         ops_launch = ops * chunks[0][1] / M  # per GEMM launch (one chunk)
         gemm_avg = statistics.mean(gemm_ms)  # per batch = sum over its chunk launches
         achieved = ops / (gemm_avg * 1e-3) / 1e12  # = ops per launch / mean launch duration
-        peak = measure_int8_peak(torch)
         traffic = None
         prof = os.path.join(ROOT, "profiles", "gemm_limb_traffic.json")
         if os.path.exists(prof):
@@ -572,7 +694,18 @@ def run_ours(args):
             lg = pj.get("limb_gemm", {})
             if lg.get("dram_bytes_per_launch") and lg.get("entries"):
                 traffic = lg["dram_bytes_per_launch"] * chunks[0][1] / lg["entries"]
-        lat_sorted = sorted(batch_ms)
+        thr_avg = statistics.mean(thr_ms)
+        mhz = clk_value.get("sm_mhz")
+        n_sm = dm.sm_count()
+        cycles = {"limb_gemm_6_engines": gemm_avg * 1e-3 * mhz * 1e6 if mhz else None,
+                  "limb_gemm_sm_mhz": mhz,
+                  "cublas_limb_gemms": (cublas_ms * 1e-3 * cublas_clk["sm_mhz"] * 1e6
+                                        if cublas_ms and cublas_clk and cublas_clk.get("sm_mhz") else None),
+                  "cublas_sm_mhz": cublas_clk.get("sm_mhz") if cublas_clk else None,
+                  "how": "CUDA-event time per batch x the median SM clock sampled during that leg "
+                         "(both arms run under the 1000 W power cap)"}
+        if cycles["limb_gemm_6_engines"] and cycles["cublas_limb_gemms"]:
+            cycles["fused_over_cublas"] = cycles["limb_gemm_6_engines"] / cycles["cublas_limb_gemms"]
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
@@ -584,9 +717,11 @@ def run_ours(args):
                        "l2": "no flush: inputs (60.4 GB share DB) exceed the 126 MB L2",
                        "parallelism": f"db-shard x{world}, 3 co-resident parties per GPU",
                        "db_chunk": chunks[0][1]},
-            "latency_ms": {"p50": lat_sorted[len(lat_sorted) // 2], "p99": lat_sorted[-1],
-                           "e2e_p50": sorted(lat)[len(lat) // 2], "e2e_p99": max(lat)},
-            "kernels_ms": {"limb_gemm_6_engines": gemm_avg, "threshold_open_or": statistics.mean(thr_ms)},
+            "latency_ms": {"p50": pct(batch_ms, 50), "p99": pct(batch_ms, 99), "of": f"the {args.steps} timed steps",
+                           "e2e_p50": pct(lat, 50), "e2e_p99": pct(lat, 99)},
+            "kernels_ms": {"limb_gemm_6_engines": gemm_avg, "threshold_open_or": thr_avg},
+            "cycles_per_batch": cycles,
+            "rows_x_entries_per_s": NQ * 31 * M * world / (per_step * 1e-3),
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": None, "unit": "TOPS",
                          "frac": None, "traffic": traffic,
                          "kernel": f"limb_gemm_kernel<256> (6 engines, one launch per {chunks[0][1]}-entry "
@@ -603,15 +738,22 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 2 * len(chunks) * args.steps,
             "gpu_launches_e2e": (2 * len(chunks) + 7) * args.steps,
-            "clocks": clk.summary(clk.windows[0]),
-            "clocks_e2e": clk.summary(clk.windows[1]),
+            "clocks": clk_value,
+            "clocks_e2e": clk_e2e,
             "planted_matches_found": f"{planted_found}/{len(planted)}",
             "setup_s": {"synth_db": synth_s},
         }
+        result["roofline_threshold"] = threshold_roofline(thr_avg, M * NQ, n_sm, mhz, chunks)
+        if fused:
+            result["fused_scan"] = fused
+        if latency:
+            result["latency"] = latency
         if batched:
             result["batched"] = batched
         if serving:
             result["serving"] = serving
+        if sweep:
+            result["sweep"] = sweep
         mp = measured_peaks()
         rf = result["roofline"]
         if mp["present"]:
@@ -636,13 +778,45 @@ def run_ours(args):
             result["cpu_baseline"] = cpu_baseline()
         print(json.dumps(result), flush=True)
 
-    for o in ce + me + [c, dc]:
-        o.close()
     dm.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def threshold_roofline(thr_ms: float, words: int, n_sm: int, sm_mhz, chunks) -> dict:
+    """Roofline of the fused threshold kernel per batch.  It is bound by its
+    integer instruction issue (ChaCha12 and the bit-sliced adders), not by
+    HBM: one thread evaluates one 32-element word, so the thread instructions
+    per word come from an ncu count of the same kernel
+    (profiles/threshold_bitmap_counters.json, smsp__inst_executed per warp),
+    and the ceiling is one warp instruction per SM sub-partition per clock:
+    SMs x 4 x 32 lanes x the SM clock sampled during the timed steps.  The HBM
+    fraction (its 6 x 64 bytes of dot shares read per word) is given beside."""
+    out = {"bound": "alu", "unit": "thread instructions/s", "words_per_batch": words,
+           "words_per_s": words / (thr_ms * 1e-3), "ms_per_batch": thr_ms,
+           "kernel": f"threshold_bitmap_kernel<128, 3> ({len(chunks)} launches per batch)",
+           "achieved": None, "peak": None, "frac": None, "inst_per_word": None}
+    prof = os.path.join(ROOT, "profiles", "threshold_bitmap_counters.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            pj = json.load(f)
+        ipw = pj.get("inst_per_word")
+        out["inst_per_word"] = ipw
+        out["counters_source"] = pj.get("source")
+        if ipw:
+            out["achieved"] = ipw * words / (thr_ms * 1e-3)
+    if sm_mhz:
+        out["peak"] = n_sm * 4 * 32 * sm_mhz * 1e6
+        out["peak_source"] = f"{n_sm} SMs x 4 sub-partitions x 32 lanes x {sm_mhz:.0f} MHz (median sampled clock)"
+        if out["achieved"]:
+            out["frac"] = out["achieved"] / out["peak"]
+    hbm = measured_peaks()["hbm_gbs"] or 6650.0
+    out["hbm_bytes_per_batch"] = words * 6 * 64
+    out["hbm_gbs"] = words * 6 * 64 / (thr_ms * 1e-3) / 1e9
+    out["frac_hbm"] = out["hbm_gbs"] / hbm
+    return out
 
 
 def _latency_stats(comps, requests, t0, db_lens):
@@ -785,11 +959,121 @@ def run_serving(args):
     dm.close()
 
 
-def run_sweep(args):
-    """Single-party limb GEMM over query rows x DB entries (K = 12800, as the
-    reference's matmul bench) and the 3-party comparison kernel over element
-    counts, each against its roofline."""
+def sweep_leg(dm, clk, min_s: float = 1.0) -> dict:
+    """The GEMM / comparison roofline sweep (configuration 2), each row timed
+    with CUDA events over at least `min_s` seconds of back-to-back launches so
+    that it carries its own clock record.
+
+    GEMM: one party's code engine (K = 12800, no zero-share mask: the
+    reference's matmul bench engine has no comms) over query rows Q x DB
+    entries M, Q in {64, 256, 1024} x M in {256K, 1M, 2M} at the library's
+    tile, the other tile width at 1M entries for Q = 256 and 1024, and the
+    reference bench's job (iris-mpc-gpu/benches/matmul.rs:17-20: 8 x 300,000
+    entries x 930 rows, spread over 8 GPUs there) on one GPU.  Bound: streaming
+    the DB (3 Q int8 ops per DB byte at the measured HBM bandwidth) or 2 x the
+    measured dense bf16 burst peak (int8 issues at twice the bf16 rate),
+    whichever is lower.
+
+    Comparison: compare_threshold_masked_many (flat) over 2^20, 2^25 and 2^30
+    elements of three parties' u16 code and mask shares."""
     import numpy as np
+    import torch
+
+    import irisb200
+
+    s0 = torch.cuda.ExternalStream(dm.stream(0), device=torch.device("cuda", dm.device))
+    mp = measured_peaks()
+    hbm = (mp["hbm_gbs"] or 6650.0) * 1e9
+    int8_peak = 2 * (mp["bf16_tflops"] or 1590.0) * 1e12
+    peak_source = ("MEASURED_PEAKS.json: 2 x bf16 burst (bf16_tflops), hbm_gbs" if mp["hbm_gbs"] and mp["bf16_tflops"]
+                   else "fallback for missing MEASURED_PEAKS.json figures: 6650 GB/s, 2 x 1590 TFLOP/s bf16 burst")
+
+    def timed(fn):
+        """(ms per launch, launches, clock record) over >= min_s seconds."""
+        fn()
+        dm.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s0)
+        fn()
+        b.record(s0)
+        b.synchronize()
+        est = max(a.elapsed_time(b), 1e-3)
+        reps = max(3, int(min_s * 1e3 / est) + 1)
+        with clk.mark():
+            a.record(s0)
+            for _ in range(reps):
+                fn()
+            b.record(s0)
+            b.synchronize()
+        return a.elapsed_time(b) / reps, reps, clk.summary(clk.windows[-1])
+
+    seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
+    K256, K1M, K2M, KREF = 262144, 1048576, 2097152, 2400000
+    rows_plan = [(q, m, 0) for q in (64, 256, 1024) for m in (K256, K1M, K2M)]
+    rows_plan += [(256, K1M, 256), (1024, K1M, 128), (930, KREF, 0)]
+    eng = irisb200.ShareDB(0, dm, KREF, 1024, K_CODE, seeds[0], is_remote=False)
+    gemm = []
+    try:
+        eng.alloc_db(KREF)
+        eng.fill_random(DB_SEED, KREF)
+        rng = np.random.default_rng(5)
+        cur_q = None
+        for q, m, tile in sorted(rows_plan, key=lambda r: (r[0], r[2], r[1])):
+            if q != cur_q:
+                eng.query_upload(rng.integers(0, 65536, (q, K_CODE), dtype=np.uint16))
+                cur_q = q
+            eng.set_tile(tile)
+            t, reps, ck = timed(lambda: eng.dot(0, m, 1, dm.stream(0)))
+            ops = 6 * K_CODE * q * m
+            hbm_bound = 3 * q * hbm
+            bound = min(int8_peak, hbm_bound)
+            row = {"query_rows": q, "db_entries": m, "tile": tile or "auto", "ms": t, "launches": reps,
+                   "tops": ops / t / 1e9, "comparisons_per_s": m * q / 31 / (t * 1e-3),
+                   "bound": "hbm" if hbm_bound < int8_peak else "tensor", "bound_tops": bound / 1e12,
+                   "frac": ops / (t * 1e-3) / bound, "clocks": ck}
+            if ck.get("sm_mhz"):
+                row["ops_per_sm_cycle"] = ops / (t * 1e-3) / (ck["sm_mhz"] * 1e6) / dm.sm_count()
+            if (q, m) == (930, KREF):
+                row["what"] = ("the reference matmul bench's job (2.4M entries x 930 rows x 12800) on one GPU; "
+                               "the reference spreads it over 8 GPUs (300,000 entries each)")
+            gemm.append(row)
+        eng.set_tile(0)
+    finally:
+        eng.close()
+
+    cmp_ = []
+    c = irisb200.Circuits(dm, seeds)
+    try:
+        for e in (1 << 20, 1 << 25, 1 << 30):
+            bufs = [irisb200.DeviceBuffer(dm, 2 * e) for _ in range(6)]
+            ra = [irisb200.DeviceBuffer(dm, e // 8) for _ in range(3)]
+            rb = [irisb200.DeviceBuffer(dm, e // 8) for _ in range(3)]
+            op = irisb200.DeviceBuffer(dm, e // 8)
+            try:
+                for i, b in enumerate(bufs):
+                    b.fill_random(1000 + i)
+                t, reps, ck = timed(lambda: c.compare_threshold_masked_many(bufs[:3], bufs[3:], e, 16384, ra, rb, op,
+                                                                            dm.stream(0)))
+            finally:
+                for b in bufs + ra + rb + [op]:
+                    b.free()
+            algo = e * 12 + e * 7 // 8  # 3 parties x (code + mask) u16 read; (a, b) bits x 3 + opened bits written
+            cmp_.append({"elements": e, "ms": t, "launches": reps, "elements_per_s": e / (t * 1e-3),
+                         "gbs": algo / t / 1e6, "frac_hbm": algo / (t * 1e-3) / hbm,
+                         "bound": "alu (ChaCha12 + bit-sliced circuits)", "clocks": ck})
+    finally:
+        c.close()
+    return {"gemm": gemm, "comparison": cmp_,
+            "config": {"workload": "configuration 2: single-party limb GEMM (K = 12800) over query rows x DB "
+                                   "entries; 3-party compare_threshold_masked_many over element counts",
+                       "int8_peak_tops": int8_peak / 1e12, "hbm_gbs": hbm / 1e9, "peak_source": peak_source,
+                       "min_seconds_per_row": min_s,
+                       "timing": "CUDA events around back-to-back launches on the launching stream; the DB "
+                                 "(6.7-61 GB) exceeds L2, so no flush"}}
+
+
+def run_sweep(args):
+    """The roofline sweep alone (sweep_leg) as one JSON line."""
     import torch
 
     import irisb200
@@ -798,71 +1082,14 @@ def run_sweep(args):
         return
     torch.cuda.set_device(0)
     dm = irisb200.DeviceManager(0)
-    s0 = torch.cuda.ExternalStream(dm.stream(0), device=torch.device("cuda", 0))
-    mp = measured_peaks()
-    hbm = (mp["hbm_gbs"] or 6650.0) * 1e9
-    int8_peak = 2 * (mp["bf16_tflops"] or 1590.0) * 1e12
-    peak_source = ("MEASURED_PEAKS.json: 2 x bf16 burst, hbm_gbs" if mp["hbm_gbs"] and mp["bf16_tflops"]
-                   else "fallback for missing MEASURED_PEAKS.json figures: 6650 GB/s, 2 x 1590 TFLOP/s bf16 burst")
-
-    def timed(fn, reps):
-        fn()
-        dm.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(s0)
-        for _ in range(reps):
-            fn()
-        b.record(s0)
-        b.synchronize()
-        return a.elapsed_time(b) / reps
-
     clk = ClockSampler(0).__enter__()
     time.sleep(2.0)
-    gemm = []
-    qs, ms = (64, 256, 1024), (262144, 1048576, 2097152)
-    seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
-    eng = irisb200.ShareDB(0, dm, max(ms), max(qs), K_CODE, seeds[0])
-    eng.alloc_db(max(ms))
-    eng.fill_random(DB_SEED, max(ms))
-    rng = np.random.default_rng(5)
-    for q in qs:
-        eng.query_upload(rng.integers(0, 65536, (q, K_CODE), dtype=np.uint16))
-        for m in ms:
-            with clk.mark():
-                t = timed(lambda: eng.dot(0, m, 1, dm.stream(0)), 3)
-            ops = 6 * K_CODE * q * m
-            bound = min(int8_peak, 3 * q * hbm)
-            gemm.append({"query_rows": q, "db_entries": m, "ms": t, "tops": ops / t / 1e9,
-                         "bound": "hbm" if 3 * q * hbm < int8_peak else "tensor",
-                         "frac": ops / (t * 1e-3) / bound, "clocks": clk.summary(clk.windows[-1])})
-    eng.close()
-    cmp_ = []
-    c = irisb200.Circuits(dm, seeds)
-    for e in (1 << 20, 1 << 23, 1 << 27, 1 << 30):
-        bufs = [irisb200.DeviceBuffer(dm, 2 * e) for _ in range(6)]
-        for i, b in enumerate(bufs):
-            b.fill_random(1000 + i)
-        ra = [irisb200.DeviceBuffer(dm, e // 8) for _ in range(3)]
-        rb = [irisb200.DeviceBuffer(dm, e // 8) for _ in range(3)]
-        op = irisb200.DeviceBuffer(dm, e // 8)
-        with clk.mark():
-            t = timed(lambda: c.compare_threshold_masked_many(bufs[:3], bufs[3:], e, 16384, ra, rb, op,
-                                                              dm.stream(0)), 3)
-        algo = e * 12 + e * 7 // 8  # 3 parties x (code + mask) u16 read; (a, b) bits x 3 + opened bits written
-        cmp_.append({"elements": e, "ms": t, "elements_per_s": e / (t * 1e-3), "gbs": algo / t / 1e6,
-                     "frac_hbm": algo / (t * 1e-3) / hbm, "bound": "alu (ChaCha12 + bit-sliced circuits)",
-                     "clocks": clk.summary(clk.windows[-1])})
-        for b in bufs + ra + rb + [op]:
-            b.free()
-    c.close()
-    clk.__exit__(None, None, None)
+    try:
+        sw = sweep_leg(dm, clk, args.sweep_seconds)
+    finally:
+        clk.__exit__(None, None, None)
     print(json.dumps({"metric": "limb GEMM TOPS and comparison elements/s (roofline sweep)", "value": None,
-                      "unit": "TOPS", "n_gpus": 1, "data": "synthetic",
-                      "config": {"workload": "single-party limb GEMM, K = 12800, query rows x DB entries; "
-                                             "3-party compare_threshold_masked_many over element counts",
-                                 "int8_peak_tops": int8_peak / 1e12, "hbm_gbs": hbm / 1e9,
-                                 "peak_source": peak_source},
-                      "gemm": gemm, "comparison": cmp_}), flush=True)
+                      "unit": "TOPS", "n_gpus": 1, "data": "synthetic", **sw}), flush=True)
     dm.close()
 
 

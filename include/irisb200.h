@@ -262,6 +262,11 @@ int irs_mirror_query_share(uint16_t* coefs, size_t n, int flip_imaginary);
  * rows) or 256 (above) when the query capacity allows; the extra rows are zero.
  * Default: the 128-row tile up to 768 padded rows, else the 256-row tile. */
 int irs_sharedb_set_tile(irs_sharedb* db, int block_n);
+/* on != 0: the 256-row tile runs as the two-SM GEMM (a cluster of two CTAs
+ * with tcgen05.mma.cta_group::2 on a 256-entry x 256-row tile; same results).
+ * Off by default: under the B200's power cap it trades clock for MAC rate, so
+ * the batch autotuner decides (no counterpart in the reference). */
+int irs_sharedb_set_pair(irs_sharedb* db, int on);
 int irs_sharedb_use_batch_counter(irs_sharedb* db, int on);
 /* Starts a new batch: the zero-share mask and circuit keystreams are drawn at
  * ChaCha counter (batch_id << 40) | position (ChaChaCtx counter,
@@ -392,6 +397,23 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
                                            irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3],
                                            size_t offset, size_t len, uint32_t threshold_a, int self_check,
                                            void* stream);
+/* The six limb GEMMs (irs_sharedb_dot_many with multipliers {1,1,1,2,2,2})
+ * and irs_dc_compare_threshold_open over entries [offset, offset+len) in ONE
+ * persistent kernel: per 128-entry x 128-row tile the six engines' masked dot
+ * shares go to an L2-resident ring slot of the CTA (never to the engines'
+ * result buffers) and the same CTA runs the threshold, open and rotation OR
+ * on them (the reference's per-chunk Phase 1 + Phase 2 + open,
+ * iris-mpc-gpu/src/server/actor.rs:2376-2519).  Plain slots (use_segments = 0:
+ * n_slots 32-row slots, rows 0..30 valid, slot s reported as query s) or the
+ * stored segment table (use_segments = 1, n_slots ignored).  Results equal the
+ * two-launch path's bit for bit.  Needs the padded query rows in multiples of
+ * 128.  The first call allocates the comparator's ring (n_SMs x 196,608
+ * bytes; a call with len = 0 only allocates), so make it before any graph
+ * capture; later calls are graph-capturable.  Afterwards the engines hold no
+ * dot shares (irs_sharedb_fetch_results refuses). */
+int irs_dc_scan_fused(irs_distance_comparator* dc, irs_circuits* c, irs_sharedb* const code_engines[3],
+                      irs_sharedb* const mask_engines[3], size_t offset, size_t len, size_t n_slots,
+                      uint32_t threshold_a, int use_segments, void* stream);
 /* Match lists of selected bitmap rows (the per-query assembly of
  * fetch_final_results, distance_comparator.rs, for rows chosen by the caller):
  * counts[i] = set bits of row rows[i] below db_len, ids [n][IRS_MAX_MATCHES_LEN]

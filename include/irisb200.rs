@@ -84,6 +84,7 @@ extern "C" {
         n: usize) -> c_int;
     pub fn irs_mirror_query_share(coefs: *mut u16, n: usize, flip_imaginary: c_int) -> c_int;
     pub fn irs_sharedb_set_tile(db: *mut IrsShareDb, block_n: c_int) -> c_int;
+    pub fn irs_sharedb_set_pair(db: *mut IrsShareDb, on: c_int) -> c_int;
     pub fn irs_sharedb_use_batch_counter(db: *mut IrsShareDb, on: c_int) -> c_int;
     pub fn irs_sharedb_set_batch(db: *mut IrsShareDb, batch_id: u64) -> c_int;
     pub fn irs_sharedb_dot(db: *mut IrsShareDb, offset: usize, len: usize, multiplier: u16,
@@ -127,6 +128,9 @@ extern "C" {
         c: *mut IrsCircuits, code_engines: *const *mut IrsShareDb,
         mask_engines: *const *mut IrsShareDb, offset: usize, len: usize, threshold_a: u32,
         self_check: c_int, stream: *mut c_void) -> c_int;
+    pub fn irs_dc_scan_fused(dc: *mut IrsDistanceComparator, c: *mut IrsCircuits,
+        code_engines: *const *mut IrsShareDb, mask_engines: *const *mut IrsShareDb, offset: usize,
+        len: usize, n_slots: usize, threshold_a: u32, use_segments: c_int, stream: *mut c_void) -> c_int;
     pub fn irs_dc_take_rows(dc: *mut IrsDistanceComparator, rows: *const u32, n: usize,
         db_len: usize, clear: c_int, counts: *mut u32, ids: *mut u32) -> c_int;
     pub fn irs_dc_enable_distance_capture(dc: *mut IrsDistanceComparator, cap: usize) -> c_int;

@@ -20,6 +20,7 @@
 #include "../../include/irisb200.h"
 #include "or_tree.h"
 #include "common.cuh"
+#include "fused_scan.h"
 #include "gemm_limb.h"
 #include "internal.h"
 #include "prep.h"
@@ -125,6 +126,7 @@ struct irs_sharedb {
   size_t n_cap = 0;          // query row capacity
   size_t rows_uploaded = 0;  // rows of the last upload
   int tile_override = 0;     // tile width requested by irs_sharedb_set_tile (0 = auto)
+  bool pair = false;         // two-SM GEMM for the 256-row tile (irs_sharedb_set_pair)
   bool batch_from_device = false;
   bool have_query = false;
   // results [max_db][n_pad] u16 (entry-major)
@@ -169,6 +171,9 @@ struct irs_distance_comparator {
   uint32_t* d_seg_mask = nullptr;   // [seg_cap]
   size_t seg_cap = 0, n_seg_slots = 0;
   bool have_segments = false;
+  // dot-share ring of the fused scan (irs_dc_scan_fused), allocated on first use
+  uint16_t* ring = nullptr;
+  size_t ring_bytes = 0;
 };
 
 namespace {
@@ -212,7 +217,7 @@ ChaChaKey key_of(const uint32_t k[8]) {
 // a query tile per CTA).
 int rebuild_query_maps(irs_sharedb* db) {
   if (db->block_n <= 0) return IRS_OK;  // no valid tile width: dot reports it
-  const uint32_t q_box = (uint32_t)(gemm_use_pair(db->block_n) ? db->block_n / 2 : db->block_n);
+  const uint32_t q_box = (uint32_t)(gemm_pair_applies(db->pair, db->block_n) ? db->block_n / 2 : db->block_n);
   if (make_tmap_u8(&db->tm_q_lo, db->q_lo, db->n_cap, db->code_length, q_box) ||
       make_tmap_u8(&db->tm_q_hi, db->q_hi, db->n_cap, db->code_length, q_box))
     return fail(IRS_ERR_CUDA, "tensor map for the query planes failed");
@@ -888,6 +893,13 @@ int irs_sharedb_set_tile(irs_sharedb* db, int block_n) {
   return IRS_OK;
 }
 
+int irs_sharedb_set_pair(irs_sharedb* db, int on) {
+  CHECK(db, IRS_ERR_INVALID, "db is NULL");
+  const bool rebuild = db->pair != (on != 0) && db->block_n == 256;
+  db->pair = on != 0;
+  return rebuild ? rebuild_query_maps(db) : IRS_OK;
+}
+
 int irs_sharedb_set_batch(irs_sharedb* db, uint64_t batch_id) {
   CHECK(db, IRS_ERR_INVALID, "db is NULL");
   CHECK(batch_id < (1ull << 24), IRS_ERR_INVALID, "batch id must be below 2^24");
@@ -935,6 +947,7 @@ int irs_sharedb_dot_many(irs_sharedb* const* engines, const uint16_t* multiplier
   for (int i = 0; i < n; i++) {
     CHECK(engines[i] && engines[i]->dm == dm, IRS_ERR_INVALID, "engine %d missing or on another device", i);
     CHECK(engines[i]->block_n == engines[0]->block_n, IRS_ERR_INVALID, "engines need the same padded query length");
+    CHECK(engines[i]->pair == engines[0]->pair, IRS_ERR_INVALID, "engines need the same GEMM variant (set_pair)");
     int rc = fill_problem(engines[i], multipliers[i], offset, len, P.prob[i]);
     if (rc) return rc;
   }
@@ -954,7 +967,7 @@ int irs_sharedb_dot_many(irs_sharedb* const* engines, const uint16_t* multiplier
       dm->stall_limit_ns = 0;
     }
     StageTimer timer(dm, s, "dot");
-    CU(launch_limb_gemm(P, engines[0]->block_n, dm->n_sms, s));
+    CU(launch_limb_gemm(P, engines[0]->block_n, engines[0]->pair, dm->n_sms, s));
   }
   for (int i = 0; i < n; i++) {
     engines[i]->res_offset = offset;
@@ -1283,7 +1296,8 @@ int irs_dc_destroy(irs_distance_comparator* dc) {
   cudaSetDevice(dc->dm->device);
   void* ps[] = {dc->bitmap, dc->self_bitmap, dc->match_list, dc->counters, dc->partial, dc->final_results,
                 dc->match_counters, dc->all_matches, dc->d_slot_valid, dc->d_slot_query,
-                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask, dc->d_take, dc->d_dist, dc->d_forced};
+                dc->d_seg_start, dc->d_seg_query, dc->d_seg_mask, dc->d_take, dc->d_dist, dc->d_forced,
+                dc->ring};
   for (void* p : ps) if (p) cudaFree(p);
   delete dc;
   return IRS_OK;
@@ -1441,6 +1455,107 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
   {
     StageTimer timer(dm, s, "threshold_open");
     CU(launch_threshold_bitmap(P, s));
+  }
+  return IRS_OK;
+}
+
+int irs_dc_scan_fused(irs_distance_comparator* dc, irs_circuits* c, irs_sharedb* const code_engines[3],
+                      irs_sharedb* const mask_engines[3], size_t offset, size_t len, size_t n_slots,
+                      uint32_t threshold_a, int use_segments, void* stream) {
+  CHECK(dc && c && code_engines && mask_engines, IRS_ERR_INVALID, "bad arguments");
+  CHECK(offset % 32 == 0, IRS_ERR_INVALID, "offset must be a multiple of 32");
+  irs_sharedb* eng[kFusedEngines] = {code_engines[0], code_engines[1], code_engines[2],
+                                      mask_engines[0], mask_engines[1], mask_engines[2]};
+  for (int e = 0; e < kFusedEngines; e++) {
+    CHECK(eng[e] && eng[e]->dm == dc->dm, IRS_ERR_INVALID, "engine %d missing or on another device", e);
+    CHECK(eng[e]->peer == e % 3, IRS_ERR_INVALID, "engine %d must belong to party %d", e, e % 3);
+    CHECK(eng[e]->code_length == (size_t)(e < 3 ? kIrisCodeLength : kMaskCodeLength), IRS_ERR_INVALID,
+          "engine %d has code length %zu", e, eng[e]->code_length);
+  }
+  const size_t n_pad = eng[0]->n_pad;
+  for (int e = 1; e < kFusedEngines; e++)
+    CHECK(eng[e]->n_pad == n_pad, IRS_ERR_INVALID, "engines need the same query padding");
+  CHECK(n_pad % kFusedBlockN == 0, IRS_ERR_INVALID,
+        "the fused scan needs padded query rows in multiples of %d (got %zu)", kFusedBlockN, n_pad);
+  if (use_segments) {
+    CHECK(dc->have_segments, IRS_ERR_STATE, "irs_dc_set_segments not called");
+    n_slots = dc->n_seg_slots;
+  } else {
+    CHECK(n_slots <= dc->max_queries && n_slots <= dc->slot_cap, IRS_ERR_INVALID, "too many slots");
+  }
+  CHECK(n_slots * kSlotRows <= n_pad, IRS_ERR_INVALID, "slots exceed the padded query rows");
+  CHECK(offset + len <= dc->stride_bits, IRS_ERR_INVALID, "entries exceed the bitmap width");
+  irs_device_manager* dm = dc->dm;
+  CU(cudaSetDevice(dm->device));
+  cudaStream_t s = party_stream(dm, 0, stream);
+  FusedParams F;
+  memset(&F, 0, sizeof F);
+  const uint16_t mults[kFusedEngines] = {1, 1, 1, 2, 2, 2};
+  for (int e = 0; e < kFusedEngines; e++) {
+    int rc = fill_problem(eng[e], mults[e], offset, len, F.prob[e]);
+    if (rc) return rc;
+    // the fused kernel's query tile is 128 rows whatever the engine's own tile width
+    if (make_tmap_u8(&F.prob[e].tm_b_lo, eng[e]->q_lo, eng[e]->n_cap, eng[e]->code_length, kFusedBlockN) ||
+        make_tmap_u8(&F.prob[e].tm_b_hi, eng[e]->q_hi, eng[e]->n_cap, eng[e]->code_length, kFusedBlockN))
+      return fail(IRS_ERR_CUDA, "tensor map for the query planes failed");
+  }
+  F.tiles_m = (int)((len + 127) / 128);
+  F.tiles_n = (int)(n_pad / kFusedBlockN);
+  F.total_work = F.tiles_m * F.tiles_n;
+  F.err = dm->d_err;
+  const size_t need = (size_t)dm->n_sms * kFusedRingBytesPerCta;  // the grid never exceeds one CTA per SM
+  if (need > dc->ring_bytes) {
+    // scratch for the dot shares of the CTAs' current tiles; allocated outside any capture
+    CHECK(!dm->capturing, IRS_ERR_STATE,
+          "the first fused scan of a comparator (which allocates its %zu-byte ring) must come before a graph capture",
+          need);
+    if (dc->ring) CU(cudaFree(dc->ring));
+    dc->ring = nullptr;
+    dc->ring_bytes = 0;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(IRS_ERR_NOMEM, "fused scan ring of %zu bytes: %s", need, cudaGetErrorString(e));
+    }
+    dc->ring = static_cast<uint16_t*>(p);
+    dc->ring_bytes = need;
+  }
+  F.ring = dc->ring;
+  ThresholdParams& T = F.T;
+  base_params(c, T);
+  T.threshold_a = threshold_a;
+  T.n_entries = (uint32_t)len;
+  T.m0 = (uint32_t)offset;
+  T.n_pad = (uint32_t)n_pad;
+  T.n_slots = (uint32_t)n_slots;
+  if (use_segments) {
+    T.seg_start = dc->d_seg_start;
+    T.seg_query = dc->d_seg_query;
+    T.seg_mask = dc->d_seg_mask;
+  } else {
+    CHECK(n_slots <= dc->max_queries, IRS_ERR_INVALID, "more slots than queries");
+  }
+  T.bitmap = dc->bitmap;
+  T.bitmap_stride = (uint32_t)dc->stride_bits;
+  T.match_count = dc->counters;
+  T.match_list = dc->match_list;
+  T.match_cap = (uint32_t)dc->match_cap;
+  set_distance_capture(dc, T);
+  // The engines' inputs may have been written on their own party streams.
+  for (int e = 0; e < kFusedEngines; e++)
+    if (!dm->capturing && dm->streams[eng[e]->peer] != s) {
+      CU(cudaEventRecord(eng[e]->done, dm->streams[eng[e]->peer]));
+      CU(cudaStreamWaitEvent(s, eng[e]->done, 0));
+    }
+  if (len && n_slots) {
+    StageTimer timer(dm, s, "scan_fused");
+    CU(launch_fused_scan(F, dm->n_sms, s));
+  }
+  for (int e = 0; e < kFusedEngines; e++) {
+    eng[e]->res_offset = offset;
+    eng[e]->res_len = 0;  // the dot shares stayed in the ring: no buffered results
+    if (!dm->capturing) CU(cudaEventRecord(eng[e]->done, s));
   }
   return IRS_OK;
 }

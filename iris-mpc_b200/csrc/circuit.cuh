@@ -54,7 +54,7 @@ IRS_HD Comp cand(Comp x, Comp y, uint32_t k0, uint32_t k1, uint32_t k2) {
 // circuit draws 24 blocks per word, and one shared copy of the ChaCha code
 // keeps the kernel's instruction working set inside the instruction cache.
 #ifdef __CUDACC__
-__host__ __device__ __noinline__
+static __host__ __device__ __noinline__
 #else
 static
 #endif
@@ -166,13 +166,17 @@ IRS_HD void slice16(const uint32_t w[16], uint32_t P[16]) {
   for (int k = 0; k < 16; k++) P[k] = A[k];
 }
 
-// Loads 32 consecutive u16 (64 bytes, 16-byte aligned) as 16 packed words.
+// Loads 32 consecutive u16 (64 bytes, 16-byte aligned) as 16 packed words:
+// through the read-only path, or (COHERENT) as ordinary loads, for data that
+// other threads of the same CTA wrote before a barrier (the read-only path is
+// not coherent with writes of the running kernel).
+template <bool COHERENT = false>
 IRS_HD void load32(const uint16_t* p, uint32_t w[16]) {
   const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
   for (int i = 0; i < 4; i++) {
 #ifdef __CUDA_ARCH__
-    uint4 v = __ldg(q + i);
+    uint4 v = COHERENT ? q[i] : __ldg(q + i);
 #else
     uint4 v = q[i];
 #endif
@@ -326,7 +330,7 @@ IRS_HD void lift_word(const uint16_t* const mask[3], WordRand& wr, uint16_t corr
 // mask[p] point at party p's own additive components (64 bytes each).
 // Returns the opened comparison bits; msb receives the components of the
 // result (party p's shares are (msb.c_p, msb.c_{p-1})).
-template <int STAGE>
+template <int STAGE, bool COHERENT = false>
 IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* const mask[3], uint32_t threshold_a,
                                WordRand& wr, Comp& msb) {
   uint32_t X[3][32];
@@ -337,7 +341,7 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
 #pragma unroll
       for (int p = 0; p < 3; p++) {
         uint32_t w[16];
-        load32(mask[p], w);
+        load32<COHERENT>(mask[p], w);
         slice16(w, M[p]);
       }
       lift_carries(M, wr, c1, c2);
@@ -375,8 +379,8 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
 #pragma unroll
     for (int p = 0; p < 3; p++) {
       uint32_t wm[16], wc[16];
-      load32(mask[p], wm);
-      load32(code[p], wc);
+      load32<COHERENT>(mask[p], wm);
+      load32<COHERENT>(code[p], wc);
 #pragma unroll
       for (int j = 0; j < 32; j++) {
         const uint32_t m = (wm[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
@@ -391,7 +395,7 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
 #pragma unroll
     for (int p = 0; p < 3; p++) {
       uint32_t wc[16];
-      load32(code[p], wc);
+      load32<COHERENT>(code[p], wc);
 #pragma unroll
       for (int j = 0; j < 32; j++) {
         const uint32_t c = (wc[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;

@@ -56,11 +56,11 @@ int make_tmap_u8(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k, 
 // Tile width along the query rows that divides n_pad (256, 128 or 64; 0 if none).
 int gemm_block_n_for(uint32_t n_pad);
 
-// True when launch_limb_gemm runs the two-SM (cta_group::2) kernel for this
-// tile width; its query tensor maps must then use boxes of block_n / 2 rows.
-// Off unless IRS_GEMM_PAIR=1 (the one-SM kernel is faster under the power cap).
-bool gemm_use_pair(int block_n);
+// True when launch_limb_gemm runs the two-SM (cta_group::2) kernel: asked for
+// (`pair`) and the 256-row tile; its query tensor maps must then use boxes of
+// block_n / 2 rows.
+bool gemm_pair_applies(bool pair, int block_n);
 
-cudaError_t launch_limb_gemm(GemmParams& P, int block_n, int n_sms, cudaStream_t stream);
+cudaError_t launch_limb_gemm(GemmParams& P, int block_n, bool pair, int n_sms, cudaStream_t stream);
 
 }  // namespace irs

@@ -23,6 +23,7 @@
 #include <stdlib.h>
 #include "circuit.cuh"
 #include "threshold.h"
+#include "threshold_emit.cuh"
 
 namespace irs {
 
@@ -84,72 +85,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) threshold_bitmap_kernel(c
     opened = threshold_word<kStageFull>(code, mask, P.threshold_a, wr, msb);
   }
   const size_t bitmap_word = (size_t)((P.m0 + group * 32) / 32);
-  // Rotation OR of one query's rows, one ballot for the warp's 32 entries.
-  auto emit = [&](uint32_t query, uint32_t row_mask, bool shared_word) {
-    const bool match = valid && (opened & row_mask) != 0;
-    const uint32_t bits = __ballot_sync(0xFFFFFFFFu, match);
-    if (P.bitmap && lane == 0) {
-      uint32_t* w = P.bitmap + (size_t)query * (P.bitmap_stride / 32) + bitmap_word;
-      if (shared_word) {
-        if (bits) atomicOr(w, bits);
-      } else {
-        *w = bits;
-      }
-    }
-    if (P.match_list && bits) {
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(P.match_count, (uint32_t)__popc(bits));
-      base = __shfl_sync(0xFFFFFFFFu, base, 0);
-      if (match) {
-        const uint32_t pos = base + (uint32_t)__popc(bits & ((1u << lane) - 1u));
-        if (pos < P.match_cap) {
-          P.match_list[2 * pos] = query;
-          P.match_list[2 * pos + 1] = (uint32_t)m_global;
-        }
-      }
-    }
-  };
-  uint32_t rows = 0;  // valid rows of the slot (for the distance capture)
-  if (P.seg_start) {
-    const uint32_t s0 = P.seg_start[slot], s1 = P.seg_start[slot + 1];
-    for (uint32_t k = s0; k < s1; k++) {
-      emit(P.seg_query[k], P.seg_mask[k], true);
-      rows |= P.seg_mask[k];
-    }
-  } else {
-    rows = P.slot_valid ? P.slot_valid[slot] : 0x7FFFFFFFu;
-    emit(P.slot_query ? P.slot_query[slot] : slot, rows, false);
-  }
-  // Distance capture of the per-rotation matches (openResults' match
-  // distance buffers, iris-mpc-gpu/src/dot/kernel.cu:73-106): rare, so one
-  // atomic per record.
-  if (P.dist_count && valid) {
-    uint32_t hits = opened & rows;
-    // forced pairs: every valid row of a listed (query, entry) is recorded
-    for (uint32_t j = 0; j < P.n_forced; j++) {
-      if (P.forced_entry[j] != (uint32_t)m_global) continue;
-      if (P.seg_start) {
-        for (uint32_t k = P.seg_start[slot]; k < P.seg_start[slot + 1]; k++)
-          if (P.seg_query[k] == P.forced_query[j]) hits |= P.seg_mask[k];
-      } else if ((P.slot_query ? P.slot_query[slot] : slot) == P.forced_query[j]) {
-        hits |= rows;
-      }
-    }
-    while (hits) {
-      const int r = __ffs(hits) - 1;
-      hits &= hits - 1;
-      const uint32_t pos = atomicAdd(P.dist_count, 1u);
-      if (pos < P.dist_cap) {
-        P.dist_entry[pos] = (uint32_t)m_global;
-        P.dist_row[pos] = slot * 32 + (uint32_t)r;
-#pragma unroll
-        for (int p = 0; p < 3; p++) {
-          P.dist_code[(size_t)p * P.dist_cap + pos] = P.code[p][off + r];
-          P.dist_mask[(size_t)p * P.dist_cap + pos] = P.mask[p][off + r];
-        }
-      }
-    }
-  }
+  // The capture rebuilds the share pointers from `off` (rare).
+  emit_word(P, opened, valid, lane, slot, m_global, bitmap_word,
+            [&](int p, int is_mask, int r) { return (is_mask ? P.mask[p] : P.code[p])[off + r]; });
 }
 
 __global__ void __launch_bounds__(kThreshThreads) lift_flat_kernel(const ThresholdParams P, uint16_t* corr) {

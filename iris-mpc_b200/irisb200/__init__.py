@@ -101,6 +101,7 @@ _SIGS = {
     "irs_sharedb_query_upload_slots": [_vp, _vp, _sz, _vp, _sz],
     "irs_sharedb_set_batch": [_vp, _u64],
     "irs_sharedb_set_tile": [_vp, _i],
+    "irs_sharedb_set_pair": [_vp, _i],
     "irs_sharedb_use_batch_counter": [_vp, _i],
     "irs_circuits_use_batch_counter": [_vp, _i],
     "irs_device_manager_set_batch_counter": [_vp, _u64, _vp],
@@ -117,6 +118,7 @@ _SIGS = {
     "irs_mirror_query_share": [_vp, _sz, _i],
     "irs_dc_set_segments": [_vp, _sz, _vp, _vp, _vp],
     "irs_dc_compare_threshold_open_prepared": [_vp, _vp, _vp, _vp, _sz, _sz, _u32, _i, _vp],
+    "irs_dc_scan_fused": [_vp, _vp, _vp, _vp, _sz, _sz, _sz, _u32, _i, _vp],
     "irs_graph_begin_capture": [_vp],
     "irs_graph_end_capture": [_vp, C.POINTER(_vp)],
     "irs_graph_launch": [_vp, _vp],
@@ -509,6 +511,10 @@ class ShareDB:
     def set_batch(self, batch_id: int) -> None:
         _check(lib().irs_sharedb_set_batch(self.h, batch_id))
 
+    def set_pair(self, on: bool) -> None:
+        """Two-SM GEMM for the 256-row tile (irs_sharedb_set_pair)."""
+        _check(lib().irs_sharedb_set_pair(self.h, int(on)))
+
     def set_tile(self, block_n: int) -> None:
         _check(lib().irs_sharedb_set_tile(self.h, block_n))
 
@@ -667,6 +673,16 @@ class DistanceComparator:
         hm = (_vp * 3)(*[e.h for e in mask_engines])
         _check(lib().irs_dc_compare_threshold_open_prepared(self.h, circuits.h, C.cast(hc, _vp), C.cast(hm, _vp),
                                                             offset, length, threshold_a, int(self_check), stream))
+
+    def scan_fused(self, circuits: Circuits, code_engines, mask_engines, offset: int, length: int,
+                   threshold_a: int, n_slots: int = 0, use_segments: bool = False, stream=None) -> None:
+        """The six limb GEMMs and the threshold/open/rotation OR of entries
+        [offset, offset + length) in one persistent kernel (irs_dc_scan_fused):
+        plain 32-row slots 0..n_slots-1, or the stored segment table."""
+        hc = (_vp * 3)(*[e.h for e in code_engines])
+        hm = (_vp * 3)(*[e.h for e in mask_engines])
+        _check(lib().irs_dc_scan_fused(self.h, circuits.h, C.cast(hc, _vp), C.cast(hm, _vp), offset, length, n_slots,
+                                       threshold_a, int(use_segments), stream))
 
     def take_rows(self, rows, db_len: int, clear: bool = True):
         """(counts [n], ids [n][256]) of the listed bitmap rows; see irs_dc_take_rows."""

@@ -15,9 +15,11 @@ prefetch_subset share_db.rs:344-407) instead of the whole DB.
 The device work of a batch -- comparator reset, the six limb GEMMs and the
 fused threshold/open/OR per DB chunk, the result merge -- is captured once per
 layout into a CUDA graph and replayed; the ChaCha batch id comes from the
-device batch counter, so a replay draws fresh randomness.  The autotuner picks
-the tile width along the query rows and the DB chunk length per padded row
-count by timing the candidates once.
+device batch counter, so a replay draws fresh randomness.  The autotuner picks,
+per padded row count, by timing each candidate's captured pass once: the path
+(the GEMM launch then the threshold launch per chunk, the same with the two-SM
+GEMM, or the one-kernel fused GEMM + threshold scan), the GEMM's tile width
+along the query rows and the DB chunk length.
 
 A request and its mirrored variant share one uploaded base share; the row
 descriptor's mirror bit makes the device build the mirrored rotations.
@@ -170,7 +172,8 @@ class BatchedEngine:
     at code_engines[p], mask at mask_engines[p])."""
 
     def __init__(self, dm: DeviceManager, code_engines, mask_engines, circuits: Circuits, max_variants: int = 512,
-                 max_reauth: int = 512, threshold_a: int = 16384, seeds=None, autotune: bool = True):
+                 max_reauth: int = 512, threshold_a: int = 16384, seeds=None, autotune: bool = True,
+                 path: str | None = None):
         self.dm = dm
         self.ce, self.me = list(code_engines), list(mask_engines)
         self.c = circuits
@@ -196,8 +199,12 @@ class BatchedEngine:
         self._inflight = [None, None]
         self._par = 0
         self.graphs = {}
-        self.tuned = {}
+        self.tuned = {}       # padded rows -> chosen (path, tile, chunk)
+        self.tune_log = {}    # padded rows -> [(candidate, ms per DB pass)]
         self.autotune = autotune
+        if path not in (None, "split", "pair", "fused"):
+            raise ValueError("path is None (tuned), 'split', 'pair' or 'fused'")
+        self.fixed = path     # restricts the candidates to one path
 
     # -- configuration -----------------------------------------------------
     def _chunks(self, n: int, chunk: int):
@@ -208,39 +215,53 @@ class BatchedEngine:
             off += ln
         return out
 
-    def _capture(self, n_slots: int, chunk: int) -> Graph:
+    def _capture(self, n_slots: int, path: str, chunk: int) -> Graph:
         engines = self.ce + self.me
 
         def body():
             self.dc.reset()
             for off, ln in self._chunks(self.db_len, chunk):
-                dot_many(engines, MULTS, off, ln)
-                self.dc.compare_threshold_open_prepared(self.c, self.ce, self.me, off, ln, self.threshold_a)
+                if path == "fused":
+                    self.dc.scan_fused(self.c, self.ce, self.me, off, ln, self.threshold_a, use_segments=True)
+                else:
+                    dot_many(engines, MULTS, off, ln)
+                    self.dc.compare_threshold_open_prepared(self.c, self.ce, self.me, off, ln, self.threshold_a)
             self.dc.join_db_matches(self.max_variants, self.db_len)
         return Graph.capture(self.dm, body)
 
-    def _tile_candidates(self, n_rows: int):
-        """The row-count policy's tile and its narrower neighbour (the widest
-        tile wins above 768 rows, where the pass stops streaming the DB)."""
+    @staticmethod
+    def _candidates(n_rows: int, db_len: int):
+        """(path, tile, DB chunk) candidates for a padded row count.
+        path "split": the GEMM launch (tile = its query-row width) then the
+        threshold launch per chunk; "pair": the same with the two-SM GEMM on
+        the 256-row tile; "fused": the one-kernel GEMM + threshold scan
+        (128-row tiles).  The 64-row GEMM tile is a candidate up to 768 rows,
+        where the pass is close to streaming the DB."""
         n_pad = (n_rows + 63) // 64 * 64
-        widths = (256, 128) if n_pad > 768 else (128, 64)
-        return [b for b in widths if n_pad % b == 0] or [64]
+        full = (db_len + 31) // 32 * 32
+        chunks = sorted({min(full, c) for c in (131072, 65536, 32768)}, reverse=True)
+        tiles = [t for t in (256, 128, 64) if n_pad % t == 0 and (t != 64 or n_pad <= 768)] or [64]
+        out = [("split", t, ch) for t in tiles for ch in chunks]
+        if n_pad % 256 == 0:
+            out += [("pair", 256, ch) for ch in chunks]
+        if n_pad % 128 == 0:
+            out += [("fused", 128, ch) for ch in chunks]
+        return out
 
-    def _chunk_candidates(self):
-        """DB entries per GEMM + threshold launch pair.  One launch of each
-        over the whole DB ran 4% slower than alternating 65,536-entry chunks
-        on 512K-entry DBs (the power-capped clock stays higher), so the whole
-        DB is a candidate only when it is that small anyway."""
-        full = (self.db_len + 31) // 32 * 32
-        return sorted({min(full, 131072), min(full, 65536)}, reverse=True)
-
-    def _run_db_pass(self, layout: Layout, tile: int, chunk: int) -> None:
-        key = (layout.n_slots, tile, chunk, self.db_len)
+    def _configure(self, path: str, tile: int) -> None:
         for e in self.ce + self.me:
-            e.set_tile(tile)
+            e.set_pair(path == "pair")
+            e.set_tile(tile if path != "fused" else 0)
+
+    def _run_db_pass(self, layout: Layout, cand) -> None:
+        path, tile, chunk = cand
+        key = (layout.n_slots, path, tile, chunk, self.db_len)
+        self._configure(path, tile)
         g = self.graphs.get(key)
         if g is None:
-            g = self._capture(layout.n_slots, chunk)
+            if path == "fused":  # allocates the comparator's ring outside the capture
+                self.dc.scan_fused(self.c, self.ce, self.me, 0, 0, self.threshold_a, use_segments=True)
+            g = self._capture(layout.n_slots, path, chunk)
             self.graphs[key] = g
         g.launch(self.dm.stream(0))
 
@@ -248,24 +269,28 @@ class BatchedEngine:
         n_pad = (layout.n_rows + 63) // 64 * 64
         if n_pad in self.tuned:
             return self.tuned[n_pad]
-        cands = [(t, ch) for t in self._tile_candidates(layout.n_rows) for ch in self._chunk_candidates()]
+        cands = self._candidates(layout.n_rows, self.db_len)
+        if self.fixed is not None:
+            cands = [c for c in cands if c[0] == self.fixed] or cands
         if not self.autotune or len(cands) == 1:
             self.tuned[n_pad] = cands[0]
             return cands[0]
         best, best_t = None, float("inf")
-        for t, ch in cands:
-            self._run_db_pass(layout, t, ch)  # warm (and capture)
+        self.tune_log[n_pad] = []
+        for cand in cands:
+            self._run_db_pass(layout, cand)  # warm (and capture)
             self.dm.synchronize()
             # consecutive passes: the power-capped clock settles differently for
             # long launches and for alternating GEMM / threshold chunks, and a
             # single pass after idle time does not show it
             t0 = time.perf_counter()
             for _ in range(2):
-                self._run_db_pass(layout, t, ch)
+                self._run_db_pass(layout, cand)
             self.dm.synchronize()
             el = time.perf_counter() - t0
+            self.tune_log[n_pad].append((cand, el / 2 * 1e3))
             if el < best_t:
-                best, best_t = (t, ch), el
+                best, best_t = cand, el
         self.tuned[n_pad] = best
         return best
 
@@ -370,8 +395,8 @@ class BatchedEngine:
                     self.me[p].query_upload_rows(buf["umask"][p, :unb], rt)
                 ss, sq, sm = buf["useg"]
                 self.dc.set_segments(ss[:uns], sq[:unq], sm[:unq])
-                tile, chunk = self._tune(ulay)  # times candidates (synchronously) once per padded size
-                self._run_db_pass(ulay, tile, chunk)
+                cand = self._tune(ulay)  # times candidates (synchronously) once per padded size
+                self._run_db_pass(ulay, cand)
                 n = len(uniq)
                 self.dc.fetch_final_results_into(n, buf["final"][:n], buf["counters"][:n], buf["matches"][:n])
             if reauth:
@@ -384,6 +409,7 @@ class BatchedEngine:
                     self.sce[p].query_upload_rows(buf["rcode"][p, :rnb], rt)
                     self.sme[p].query_upload_rows(buf["rmask"][p, :rnb], rt)
                 for e in self.sce + self.sme:
+                    e.set_pair(False)
                     e.set_tile(0)
                 self.sdc.reset()
                 ss, sq, sm = buf["rseg"]

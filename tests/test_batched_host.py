@@ -126,7 +126,7 @@ def _fake_engine(monkeypatch):
     e.dc, e.sdc = DC(), SDC()
     e.threshold_a, e.max_variants, e.max_reauth, e.db_len = 16384, 16, 8, 4096
     e._pin, e._pinned, e._events, e._inflight, e._par = None, [], None, [None, None], 0
-    e.graphs, e.tuned, e.autotune = {}, {}, False
+    e.graphs, e.tuned, e.autotune, e.tune_log, e.fixed = {}, {}, False, {}, None
     assert MAX_MATCHES_LEN >= 1
     return e, dm
 
@@ -190,3 +190,22 @@ def test_submit_edge_batches(monkeypatch):
     res = e.run([Request(code=z[0], mask=z[1], n_rot=16)])
     assert res[0].matches == [100] and res[0].reauth_match is None and e.graphs
     e.close()
+
+
+def test_autotuner_candidates():
+    """The tuner's candidates: the two-launch path at every tile width that
+    divides the padded rows (the 64-row tile only up to 768 rows), the two-SM
+    GEMM where the 256-row tile applies, the fused scan where the rows are a
+    multiple of 128, each at 131,072 / 65,536 / 32,768-entry chunks (capped at
+    the DB)."""
+    from irisb200.batched import BatchedEngine
+    c = BatchedEngine._candidates(2048, 524288)
+    assert ("split", 256, 131072) in c and ("split", 128, 32768) in c
+    assert not any(t == 64 for _, t, _ in c)
+    assert ("pair", 256, 65536) in c and ("fused", 128, 32768) in c
+    assert len(c) == 2 * 3 + 3 + 3
+    c = BatchedEngine._candidates(640, 524288)
+    assert {t for p, t, _ in c if p == "split"} == {128, 64}
+    assert not any(p == "pair" for p, _, _ in c) and any(p == "fused" for p, _, _ in c)
+    c = BatchedEngine._candidates(64, 1000)
+    assert c == [("split", 64, 1024)]

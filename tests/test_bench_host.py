@@ -63,3 +63,25 @@ def test_measured_peaks_parsing(tmp_path, monkeypatch):
     assert mp == {"hbm_gbs": 6540.5, "bf16_tflops": 1590.0, "bf16_tflops_sustained": None, "present": True}
     (tmp_path / "MEASURED_PEAKS.json").write_text("{not json")
     assert bench.measured_peaks()["hbm_gbs"] is None
+
+
+def test_percentiles_and_threshold_roofline(tmp_path, monkeypatch):
+    """Latency percentiles are nearest-rank (p99 of 200 samples is the 198th
+    value, not the maximum); the threshold roofline takes its instructions per
+    word from the profile counters file and its ceiling from the SM count and
+    the sampled clock."""
+    import json
+    assert bench.pct(list(range(1, 201)), 99) == 198
+    assert bench.pct(list(range(1, 101)), 50) == 50
+    assert bench.pct([7.0], 99) == 7.0
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    rf = bench.threshold_roofline(10.0, 1000, 148, 1500.0, [(0, 1)])
+    assert rf["achieved"] is None and rf["frac"] is None
+    assert rf["peak"] == 148 * 4 * 32 * 1500.0e6
+    assert abs(rf["words_per_s"] - 1000 / 0.01) < 1e-6
+    (tmp_path / "profiles").mkdir()
+    (tmp_path / "profiles" / "threshold_bitmap_counters.json").write_text(
+        json.dumps({"inst_per_word": 20000.0, "source": "test"}))
+    rf = bench.threshold_roofline(10.0, 1000, 148, 1500.0, [(0, 1)])
+    assert abs(rf["achieved"] - 20000.0 * 1000 / 0.01) < 1e-3
+    assert abs(rf["frac"] - rf["achieved"] / rf["peak"]) < 1e-12
