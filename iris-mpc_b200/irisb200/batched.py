@@ -465,6 +465,9 @@ class BatchedEngine:
         for g in self.graphs.values():
             g.close()
         self.graphs.clear()
+        for e in self.ce + self.me:  # the DB engines go back to the library's default GEMM
+            e.set_pair(False)
+            e.set_tile(0)
         for o in self.sce + self.sme + [self.dc, self.sdc]:
             o.close()
         for a in self._pinned:

@@ -147,3 +147,42 @@ def test_pipelined_batches_match_one_at_a_time(dm, oracle, setup):
     finally:
         eng.close()
         c.close()
+
+
+@pytest.mark.parametrize("path", ["split", "pair", "fused"])
+def test_batched_every_tuner_candidate(dm, oracle, setup, path):
+    """Every (path, tile, chunk) candidate the autotuner may pick gives the CPU
+    path's matches: the GEMM launch + threshold launch at each tile width, the
+    two-SM GEMM, and the one-kernel fused scan."""
+    s = setup
+    c = irisb200.Circuits(dm, W.SEEDS)
+    eng = BatchedEngine(dm, s["ce"], s["me"], c, max_variants=64, max_reauth=16, threshold_a=A, autotune=False,
+                        path=path)
+    try:
+        spec = [(0, 31, False, "uniqueness", -1), (1, 16, True, "uniqueness", -1), (3, 31, True, "uniqueness", -1),
+                (4, 1, True, "uniqueness", -1), (6, 31, False, "reauth", 1000), (9, 31, True, "uniqueness", -1),
+                (8, 16, False, "uniqueness", -1)]
+        reqs = [Request(code=s["qc"][:, q], mask=s["qm"][:, q], n_rot=n, mirrored=mir, kind=k, target=t)
+                for q, n, mir, k, t in spec]
+        eng.run(reqs)  # fixes the padded row count the tuner keys on
+        (n_pad, first), = eng.tuned.items()
+        assert first[0] == path
+        cands = [cd for cd in BatchedEngine._candidates(n_pad, N_DB) if cd[0] == path]
+        assert cands
+        for cand in cands:
+            eng.tuned = {n_pad: cand}
+            res = eng.run(reqs)
+            for (q, n, mir, k, t), r in zip(spec, res):
+                qc, qm = s["qc"][:, q], s["qm"][:, q]
+                if k == "uniqueness":
+                    assert r.matches == expected_hits(oracle, s["cs"], s["ms"], qc, qm, n, False, np.arange(N_DB)), \
+                        f"{cand} query {q}"
+                    if mir:
+                        assert r.mirror_matches == expected_hits(oracle, s["cs"], s["ms"], qc, qm, n, True,
+                                                                 np.arange(N_DB)), f"{cand} mirrored query {q}"
+                else:
+                    exp = expected_hits(oracle, s["cs"], s["ms"], qc, qm, n, False, np.array([t]))
+                    assert r.reauth_match == bool(exp), f"{cand} reauth {q}->{t}"
+    finally:
+        eng.close()
+        c.close()
