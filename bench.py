@@ -93,6 +93,8 @@ def parse():
                     help="default run: batched-leg batches timed one at a time")
     ap.add_argument("--no-sweep", action="store_true", help="default run: skip the roofline sweep leg")
     ap.add_argument("--no-fused", action="store_true", help="default run: skip the fused-scan leg")
+    ap.add_argument("--plain-path", default="tuned", choices=["tuned", "split", "pair", "fused"],
+                    help="plain step: DB pass path (tuned = PlainScan.tune picks path and chunk on the batch)")
     ap.add_argument("--sweep-seconds", type=float, default=1.0,
                     help="sweep: minimum timed seconds per row (each row carries its own clock record)")
     return ap.parse_args()
@@ -404,19 +406,15 @@ def run_ours(args):
     # tensor-bound GEMM with the ALU-bound threshold at this granularity keeps
     # the power-capped clock steadier than one long launch of each (measured
     # 160 ms per batch at 65,536 entries against 167 ms whole-DB).
+    from irisb200.scan import PlainScan
+    ps = PlainScan(dm, ce, me, c, dc, NQ, M, A)
     chunk = args.db_chunk if 0 < args.db_chunk < M else M
-    chunks = [(o, min(chunk, M - o)) for o in range(0, M, chunk)]
 
     def scan(ev=None):
-        for k, (off, ln) in enumerate(chunks):
-            if ev:
-                ev[k][0].record(s0)
-            irisb200.dot_many(engines, mults, off, ln)
-            if ev:
-                ev[k][1].record(s0)
-            dc.compare_threshold_open(c, ce, me, off, ln, NQ, A)
-            if ev:
-                ev[k][2].record(s0)
+        if ev:
+            ps.scan(events=[[(lambda e=e: e.record(s0)) for e in trio] for trio in ev])
+        else:
+            ps.scan()
 
     def device_step(ev=None):
         dc.reset()
@@ -425,6 +423,14 @@ def run_ours(args):
     clk = ClockSampler(local).__enter__()
     time.sleep(2.0)  # let nvidia-smi initialise before anything is timed
     upload()
+    # The DB pass's path and chunk length: tuned on this batch (the library's
+    # PlainScan.tune), or fixed by --plain-path / --db-chunk.
+    if args.plain_path == "tuned":
+        chosen = ps.tune()
+    else:
+        ps.configure((args.plain_path, 0 if args.plain_path == "fused" else 256, chunk))
+        chosen = ps.cand
+    chunks = ps.chunks()
     for _ in range(args.warmup):
         device_step()
     dm.synchronize()
@@ -557,6 +563,7 @@ def run_ours(args):
         e2e_s = float(t.item())
     e2e_value = comps * args.steps / e2e_s
 
+    ps.restore()
     # ---------------- batched uneven leg (same engines, same DB) ----------------
     batched = None
     if reqs:
@@ -619,6 +626,8 @@ def run_ours(args):
                        "uniqueness_orientations": n_var, "reauth_orientations": n_reauth,
                        "uniqueness_query_rows": rows, "packed_rows": lay.n_rows, "comparisons_per_batch": bcomp,
                        "autotuned_tile_chunk": tuned,
+                       "autotune_ms_per_pass": {str(k): [[list(cd), round(ms, 1)] for cd, ms in v]
+                                                for k, v in eng.tune_log.items()},
                        "timing": "host wall clock per batch through BatchedEngine.run, one batch at a time "
                                  "(H2D of the shares, graph replay of the DB pass, reauth subset pass, D2H of "
                                  "the match lists)"},
@@ -692,7 +701,7 @@ def run_ours(args):
             # proportion to the entries a launch scans (one query-plane re-read per
             # sweep of the SMs over the DB slabs), so scale to this launch
             lg = pj.get("limb_gemm", {})
-            if lg.get("dram_bytes_per_launch") and lg.get("entries"):
+            if lg.get("dram_bytes_per_launch") and lg.get("entries") and chosen[0] == "split":
                 traffic = lg["dram_bytes_per_launch"] * chunks[0][1] / lg["entries"]
         thr_avg = statistics.mean(thr_ms)
         mhz = clk_value.get("sm_mhz")
@@ -716,7 +725,10 @@ def run_ours(args):
                        "padded_query_rows": n_rows, "threshold_a": A, "threshold_ratio": 0.375,
                        "l2": "no flush: inputs (60.4 GB share DB) exceed the 126 MB L2",
                        "parallelism": f"db-shard x{world}, 3 co-resident parties per GPU",
-                       "db_chunk": chunks[0][1]},
+                       "db_chunk": chunks[0][1], "db_pass_path": chosen[0],
+                       "db_pass_choice": ("PlainScan.tune on the batch: "
+                                          + "; ".join(f"{p}/{t}/{ch}: {ms:.1f} ms" for (p, t, ch), ms in ps.tune_log))
+                                         if ps.tune_log else "fixed (--plain-path)"},
             "latency_ms": {"p50": pct(batch_ms, 50), "p99": pct(batch_ms, 99), "of": f"the {args.steps} timed steps",
                            "e2e_p50": pct(lat, 50), "e2e_p99": pct(lat, 99)},
             "kernels_ms": {"limb_gemm_6_engines": gemm_avg, "threshold_open_or": thr_avg},
@@ -724,8 +736,10 @@ def run_ours(args):
             "rows_x_entries_per_s": NQ * 31 * M * world / (per_step * 1e-3),
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": None, "unit": "TOPS",
                          "frac": None, "traffic": traffic,
-                         "kernel": f"limb_gemm_kernel<256> (6 engines, one launch per {chunks[0][1]}-entry "
-                                   f"DB chunk, {len(chunks)} per batch)",
+                         "kernel": {"split": "limb_gemm_kernel<256>", "pair": "limb_gemm_pair_kernel (cta_group::2)",
+                                    "fused": "fused_scan_kernel (GEMM and threshold: time includes the threshold)"}
+                                   [chosen[0]] + f" (6 engines, one launch per {chunks[0][1]}-entry DB chunk, "
+                                   f"{len(chunks)} per batch)",
                          "ops_per_launch": ops_launch,
                          "peak_source": "2 x measured dense bf16, sustained (MEASURED_PEAKS.json "
                                         "bf16_tflops_sustained; dense int8 issues at twice the bf16 rate on "
@@ -736,8 +750,8 @@ def run_ours(args):
             "cublas_limb_gemm_ms_per_batch": cublas_ms,
             "cublas_limb_gemm_clocks": cublas_clk,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": 2 * len(chunks) * args.steps,
-            "gpu_launches_e2e": (2 * len(chunks) + 7) * args.steps,
+            "gpu_launches": (1 if chosen[0] == "fused" else 2) * len(chunks) * args.steps,
+            "gpu_launches_e2e": ((1 if chosen[0] == "fused" else 2) * len(chunks) + 7) * args.steps,
             "clocks": clk_value,
             "clocks_e2e": clk_e2e,
             "planted_matches_found": f"{planted_found}/{len(planted)}",
@@ -969,7 +983,8 @@ def sweep_leg(dm, clk, min_s: float = 1.0) -> dict:
     entries M, Q in {64, 256, 1024} x M in {256K, 1M, 2M} at the library's
     tile, the other tile width at 1M entries for Q = 256 and 1024, and the
     reference bench's job (iris-mpc-gpu/benches/matmul.rs:17-20: 8 x 300,000
-    entries x 930 rows, spread over 8 GPUs there) on one GPU.  Bound: streaming
+    entries x 930 rows, spread over 8 GPUs there) on one GPU; the two-SM
+    (cta_group::2) kernel at 1M entries for Q = 256 and 1024.  Bound: streaming
     the DB (3 Q int8 ops per DB byte at the measured HBM bandwidth) or 2 x the
     measured dense bf16 burst peak (int8 issues at twice the bf16 rate),
     whichever is lower.
@@ -1010,7 +1025,7 @@ def sweep_leg(dm, clk, min_s: float = 1.0) -> dict:
     seeds = [([0] * 8, [2] * 8), ([1] * 8, [0] * 8), ([2] * 8, [1] * 8)]
     K256, K1M, K2M, KREF = 262144, 1048576, 2097152, 2400000
     rows_plan = [(q, m, 0) for q in (64, 256, 1024) for m in (K256, K1M, K2M)]
-    rows_plan += [(256, K1M, 256), (1024, K1M, 128), (930, KREF, 0)]
+    rows_plan += [(256, K1M, 256), (1024, K1M, 128), (256, K1M, "pair"), (1024, K1M, "pair"), (930, KREF, 0)]
     eng = irisb200.ShareDB(0, dm, KREF, 1024, K_CODE, seeds[0], is_remote=False)
     gemm = []
     try:
@@ -1018,11 +1033,12 @@ def sweep_leg(dm, clk, min_s: float = 1.0) -> dict:
         eng.fill_random(DB_SEED, KREF)
         rng = np.random.default_rng(5)
         cur_q = None
-        for q, m, tile in sorted(rows_plan, key=lambda r: (r[0], r[2], r[1])):
+        for q, m, tile in sorted(rows_plan, key=lambda r: (r[0], str(r[2]), r[1])):
             if q != cur_q:
                 eng.query_upload(rng.integers(0, 65536, (q, K_CODE), dtype=np.uint16))
                 cur_q = q
-            eng.set_tile(tile)
+            eng.set_pair(tile == "pair")  # the two-SM kernel on the 256-row tile
+            eng.set_tile(256 if tile == "pair" else tile)
             t, reps, ck = timed(lambda: eng.dot(0, m, 1, dm.stream(0)))
             ops = 6 * K_CODE * q * m
             hbm_bound = 3 * q * hbm
@@ -1037,6 +1053,7 @@ def sweep_leg(dm, clk, min_s: float = 1.0) -> dict:
                 row["what"] = ("the reference matmul bench's job (2.4M entries x 930 rows x 12800) on one GPU; "
                                "the reference spreads it over 8 GPUs (300,000 entries each)")
             gemm.append(row)
+        eng.set_pair(False)
         eng.set_tile(0)
     finally:
         eng.close()

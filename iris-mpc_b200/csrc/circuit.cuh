@@ -83,10 +83,54 @@ struct WordRand {
     }
     chacha12_x3(&pre[0][0], (uint32_t)(base + (uint64_t)b), &ks[0][0]);
   }
+  // word j of stream s's current block
+  IRS_HD uint32_t k(int s, int j) const { return ks[s][j]; }
 };
 
+#ifdef __CUDACC__
+// The three streams' current blocks from prepared words-of-four in shared
+// memory, element i of this thread at pre[i * nt] (18 of them) and keystream
+// word (s, j) written to ks[(16 s + j) * nt].  Out of line for the same
+// instruction-cache reason as chacha12_x3.
+static __device__ __noinline__ void chacha12_x3_strided(const uint4* pre, uint32_t* ks, int nt, uint32_t ctr_lo) {
+#pragma unroll 1
+  for (int s = 0; s < 3; s++) {
+    const uint4* q = pre + 6 * s * nt;
+    chacha12_core(q[0], q[nt], q[2 * nt], q[3 * nt], q[4 * nt], q[5 * nt], ctr_lo, ks + 16 * s * nt, nt);
+  }
+}
+
+// WordRand with its keystream and prepared columns in shared memory instead
+// of the thread's local memory: the block's threads interleave them
+// ([element][thread], so a warp's accesses hit consecutive words and never
+// conflict), `pre` and `ks` point at this thread's column and nt is the
+// thread count of the block.  Same keystream as WordRand.
+struct WordRandShared {
+  ChaChaKey key[3];
+  uint64_t nonce;
+  uint64_t base;
+  bool prepared = false;
+  uint4* pre;    // [18][nt] words-of-four: 6 per stream
+  uint32_t* ks;  // [48][nt]: 16 per stream
+  int nt;
+  __device__ void load(int b) {
+    if (!prepared) {
+      for (int s = 0; s < 3; s++) {
+        alignas(16) uint32_t t[24];
+        chacha_prepare(key[s], (uint32_t)(base >> 32), nonce, t);
+#pragma unroll
+        for (int q = 0; q < 6; q++) pre[(6 * s + q) * nt] = make_uint4(t[4 * q], t[4 * q + 1], t[4 * q + 2], t[4 * q + 3]);
+      }
+      prepared = true;
+    }
+    chacha12_x3_strided(pre, ks, nt, (uint32_t)(base + (uint64_t)b));
+  }
+  __device__ uint32_t k(int s, int j) const { return ks[(16 * s + j) * nt]; }
+};
+#endif
+
 // Gate g (compile-time after unrolling) must lie in the loaded block.
-#define IRS_GATE(wr, x, y, g) cand((x), (y), (wr).ks[0][(g) & 15], (wr).ks[1][(g) & 15], (wr).ks[2][(g) & 15])
+#define IRS_GATE(wr, x, y, g) cand((x), (y), (wr).k(0, (g) & 15), (wr).k(1, (g) & 15), (wr).k(2, (g) & 15))
 
 // Byte select from the pair (a, b): result byte i = byte ((sel >> 4i) & 7)
 // of the 8-byte value b:a (one PRMT on the device).
@@ -187,7 +231,8 @@ IRS_HD void load32(const uint16_t* p, uint32_t w[16]) {
 // binary_add_3_get_two_carries for K = 16 on the three components of a
 // 16-bit value (M[p][k] = plane k of component p).  Returns the carries c1
 // (bit 16) and c2 (bit 17) of M0 + M1 + M2.
-IRS_HD void lift_carries(const uint32_t M[3][16], WordRand& wr, Comp& c1, Comp& c2) {
+template <class WR>
+IRS_HD void lift_carries(const uint32_t M[3][16], WR& wr, Comp& c1, Comp& c2) {
   // carry-save: s = x1^x2^x3 = (M0, M1, M2); c = AND(x1^x3, x2^x3) ^ x3
   Comp carry = {0, 0, 0};
   Comp b_prev = {0, 0, 0};
@@ -221,7 +266,8 @@ IRS_HD void lift_carries(const uint32_t M[3][16], WordRand& wr, Comp& c1, Comp& 
 
 // binary_add_3_get_msb on the three components of a 32-bit value
 // (P[p][k] = plane k of component p).  Returns the components of bit 31.
-IRS_HD Comp msb_of_sum(const uint32_t P[3][32], WordRand& wr) {
+template <class WR>
+IRS_HD Comp msb_of_sum(const uint32_t P[3][32], WR& wr) {
   Comp carry = {0, 0, 0};
   Comp a30 = {0, 0, 0}, b30 = {0, 0, 0};
 #pragma unroll
@@ -330,9 +376,9 @@ IRS_HD void lift_word(const uint16_t* const mask[3], WordRand& wr, uint16_t corr
 // mask[p] point at party p's own additive components (64 bytes each).
 // Returns the opened comparison bits; msb receives the components of the
 // result (party p's shares are (msb.c_p, msb.c_{p-1})).
-template <int STAGE, bool COHERENT = false>
+template <int STAGE, bool COHERENT = false, class WR>
 IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* const mask[3], uint32_t threshold_a,
-                               WordRand& wr, Comp& msb) {
+                               WR& wr, Comp& msb) {
   uint32_t X[3][32];
   if (STAGE == kStageFull) {
     Comp c1, c2;
@@ -359,8 +405,8 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
       wr.load(6);
 #pragma unroll 1
       for (int i = 0; i < 16; i++)
-        inject_pair((w0 >> i) & 0x00010001u, (w1 >> i) & 0x00010001u, (w2 >> i) & 0x00010001u, wr.ks[0][i],
-                    wr.ks[1][i], wr.ks[2][i], corr[0][i], corr[1][i], corr[2][i]);
+        inject_pair((w0 >> i) & 0x00010001u, (w1 >> i) & 0x00010001u, (w2 >> i) & 0x00010001u, wr.k(0, i),
+                    wr.k(1, i), wr.k(2, i), corr[0][i], corr[1][i], corr[2][i]);
     }
     {
       const uint32_t w0 = unzip_bits(c2.c0), w1 = unzip_bits(c2.c1), w2 = unzip_bits(c2.c2);
@@ -368,8 +414,8 @@ IRS_HD uint32_t threshold_word(const uint16_t* const code[3], const uint16_t* co
 #pragma unroll 1
       for (int i = 0; i < 16; i++) {
         uint32_t a[3];
-        inject_pair((w0 >> i) & 0x00010001u, (w1 >> i) & 0x00010001u, (w2 >> i) & 0x00010001u, wr.ks[0][i],
-                    wr.ks[1][i], wr.ks[2][i], a[0], a[1], a[2]);
+        inject_pair((w0 >> i) & 0x00010001u, (w1 >> i) & 0x00010001u, (w2 >> i) & 0x00010001u, wr.k(0, i),
+                    wr.k(1, i), wr.k(2, i), a[0], a[1], a[2]);
 #pragma unroll
         for (int p = 0; p < 3; p++) corr[p][i] = add2(corr[p][i], (a[p] << 1) & 0xFFFEFFFEu);
       }

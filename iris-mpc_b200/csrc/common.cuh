@@ -114,12 +114,12 @@ IRS_HD void chacha_prepare(const ChaChaKey& key, uint32_t ctr_hi, uint64_t nonce
   pre[20] = x3; pre[21] = x7; pre[22] = x11; pre[23] = x15;
 }
 
-// ChaCha12 block with counter (pre's ctr_hi << 32 | ctr_lo): the same
-// keystream as chacha_block<12>, starting from the prepared columns.
-// `pre` is 16-byte aligned.
-IRS_HD void chacha12_block_prepared(const uint32_t* pre, uint32_t ctr_lo, uint32_t out[16]) {
-  const uint4* q = reinterpret_cast<const uint4*>(pre);
-  const uint4 k0 = q[0], k1 = q[1], cn = q[2], c1 = q[3], c2 = q[4], c3 = q[5];
+// ChaCha12 block with counter (ctr_hi << 32 | ctr_lo) from the six prepared
+// words-of-four of chacha_prepare (k0 = key 0..3, k1 = key 4..7, cn = ctr_hi,
+// nonce, c1..c3 = the prepared columns): the same keystream as
+// chacha_block<12>.  Word j goes to out[j * stride].
+IRS_HD void chacha12_core(uint4 k0, uint4 k1, uint4 cn, uint4 c1, uint4 c2, uint4 c3, uint32_t ctr_lo,
+                          uint32_t* out, int stride) {
   const uint32_t s0 = 0x61707865u, s1 = 0x3320646eu, s2 = 0x79622d32u, s3 = 0x6b206574u;
   uint32_t x0 = s0, x4 = k0.x, x8 = k1.x, x12 = ctr_lo;
   IRS_QR(x0, x4, x8, x12)
@@ -132,10 +132,17 @@ IRS_HD void chacha12_block_prepared(const uint32_t* pre, uint32_t ctr_lo, uint32
     IRS_QR(x0, x4, x8, x12) IRS_QR(x1, x5, x9, x13) IRS_QR(x2, x6, x10, x14) IRS_QR(x3, x7, x11, x15)
     IRS_QR(x0, x5, x10, x15) IRS_QR(x1, x6, x11, x12) IRS_QR(x2, x7, x8, x13) IRS_QR(x3, x4, x9, x14)
   }
-  out[0] = x0 + s0; out[1] = x1 + s1; out[2] = x2 + s2; out[3] = x3 + s3;
-  out[4] = x4 + k0.x; out[5] = x5 + k0.y; out[6] = x6 + k0.z; out[7] = x7 + k0.w;
-  out[8] = x8 + k1.x; out[9] = x9 + k1.y; out[10] = x10 + k1.z; out[11] = x11 + k1.w;
-  out[12] = x12 + ctr_lo; out[13] = x13 + cn.x; out[14] = x14 + cn.y; out[15] = x15 + cn.z;
+  out[0 * stride] = x0 + s0; out[1 * stride] = x1 + s1; out[2 * stride] = x2 + s2; out[3 * stride] = x3 + s3;
+  out[4 * stride] = x4 + k0.x; out[5 * stride] = x5 + k0.y; out[6 * stride] = x6 + k0.z;
+  out[7 * stride] = x7 + k0.w; out[8 * stride] = x8 + k1.x; out[9 * stride] = x9 + k1.y;
+  out[10 * stride] = x10 + k1.z; out[11 * stride] = x11 + k1.w; out[12 * stride] = x12 + ctr_lo;
+  out[13 * stride] = x13 + cn.x; out[14 * stride] = x14 + cn.y; out[15 * stride] = x15 + cn.z;
+}
+
+// chacha12_core from a contiguous prepared array pre[24] (16-byte aligned).
+IRS_HD void chacha12_block_prepared(const uint32_t* pre, uint32_t ctr_lo, uint32_t out[16]) {
+  const uint4* q = reinterpret_cast<const uint4*>(pre);
+  chacha12_core(q[0], q[1], q[2], q[3], q[4], q[5], ctr_lo, out, 1);
 }
 #undef IRS_QR
 #undef IRS_ROT16

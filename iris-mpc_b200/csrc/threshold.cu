@@ -30,19 +30,33 @@ namespace irs {
 namespace {
 
 constexpr int kThreshThreads = 128;
+// Shared memory per thread of the keystream (WordRandShared): 18 prepared
+// words-of-four and 48 keystream words.
+constexpr int kRandSmemPerThread = 18 * 16 + 48 * 4;
 
-__device__ __forceinline__ void init_rand(WordRand& wr, const ThresholdParams& P, uint64_t word_id) {
+template <class WR>
+__device__ __forceinline__ void init_rand(WR& wr, const ThresholdParams& P, uint64_t word_id) {
 #pragma unroll
   for (int s = 0; s < 3; s++) wr.key[s] = P.key[s];
   wr.nonce = P.nonce;
   wr.base = counter_of(P.batch_dev ? *P.batch_dev : P.batch, word_id * (uint64_t)kCircuitBlocksPerWord);
 }
 
+// This thread's keystream columns in the block's shared memory ([element][thread]).
+template <int THREADS>
+__device__ __forceinline__ void bind_rand(WordRandShared& wr) {
+  extern __shared__ uint4 rand_smem[];
+  wr.pre = rand_smem + threadIdx.x;
+  wr.ks = reinterpret_cast<uint32_t*>(rand_smem + 18 * THREADS) + threadIdx.x;
+  wr.nt = THREADS;
+}
+
 template <int STAGE>
 __global__ void __launch_bounds__(kThreshThreads) threshold_flat_kernel(const ThresholdParams P) {
   const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.n_words) return;
-  WordRand wr;
+  WordRandShared wr;
+  bind_rand<kThreshThreads>(wr);
   init_rand(wr, P, P.word_base + w);
   const uint16_t* code[3] = {P.code[0] + 32 * w, P.code[1] + 32 * w, P.code[2] + 32 * w};
   const uint16_t* mask[3] = {P.mask[0] + 32 * w, P.mask[1] + 32 * w, P.mask[2] + 32 * w};
@@ -72,7 +86,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) threshold_bitmap_kernel(c
   const uint32_t m_read = valid ? m_local : (P.n_entries - 1);
   const uint64_t m_global = (uint64_t)P.m0 + m_local;
 
-  WordRand wr;
+  WordRandShared wr;
+  bind_rand<THREADS>(wr);
   init_rand(wr, P, ((uint64_t)P.m0 + m_read) * (uint64_t)(P.n_pad / 32) + slot);
   const size_t off = (size_t)m_read * P.n_pad + (size_t)slot * 32;
   uint32_t opened;
@@ -110,11 +125,23 @@ __global__ void __launch_bounds__(kThreshThreads) lift_flat_kernel(const Thresho
 
 }  // namespace
 
+constexpr int kRandSmem = kThreshThreads * kRandSmemPerThread;  // 61,440 bytes per block
+
+template <class K>
+static cudaError_t allow_rand_smem(K kernel) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRandSmem);
+}
+
 cudaError_t launch_threshold_flat(const ThresholdParams& P, int stage, cudaStream_t stream) {
   if (P.n_words == 0) return cudaSuccess;
+  static cudaError_t attr = [] {
+    cudaError_t e = allow_rand_smem(threshold_flat_kernel<kStageFull>);
+    return e == cudaSuccess ? allow_rand_smem(threshold_flat_kernel<kStageMsbOnly>) : e;
+  }();
+  if (attr != cudaSuccess) return attr;
   const unsigned grid = (unsigned)((P.n_words + kThreshThreads - 1) / kThreshThreads);
-  if (stage == kStageFull) threshold_flat_kernel<kStageFull><<<grid, kThreshThreads, 0, stream>>>(P);
-  else threshold_flat_kernel<kStageMsbOnly><<<grid, kThreshThreads, 0, stream>>>(P);
+  if (stage == kStageFull) threshold_flat_kernel<kStageFull><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
+  else threshold_flat_kernel<kStageMsbOnly><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
   return cudaGetLastError();
 }
 
@@ -131,9 +158,14 @@ cudaError_t launch_threshold_bitmap(const ThresholdParams& P, cudaStream_t strea
     const char* e = getenv("IRS_THRESHOLD_WARPS_PER_SM");
     return e && atoi(e) == 8;
   }();
+  static cudaError_t attr = [] {
+    cudaError_t e = allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 2>);
+    return e == cudaSuccess ? allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 3>) : e;
+  }();
+  if (attr != cudaSuccess) return attr;
   const unsigned grid = (unsigned)((warps * 32 + kThreshThreads - 1) / kThreshThreads);
-  if (eight) threshold_bitmap_kernel<kThreshThreads, 2><<<grid, kThreshThreads, 0, stream>>>(P);
-  else threshold_bitmap_kernel<kThreshThreads, 3><<<grid, kThreshThreads, 0, stream>>>(P);
+  if (eight) threshold_bitmap_kernel<kThreshThreads, 2><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
+  else threshold_bitmap_kernel<kThreshThreads, 3><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
   return cudaGetLastError();
 }
 

@@ -164,3 +164,34 @@ def test_fused_rejects_narrow_row_padding(dm, data):
         dm.synchronize()
     finally:
         _close([dc, c] + ce + me)
+
+
+def test_plain_scan_every_candidate(dm, oracle, data):
+    """PlainScan (the plain drop-in's autotuned DB pass) gives the CPU path's
+    bitmap on every (path, tile, chunk) candidate, and tune() picks one of
+    them."""
+    from irisb200.scan import PlainScan
+    ce, me = _setup(dm, data, N_Q * 32)
+    c = irisb200.Circuits(dm, W.SEEDS)
+    dc = irisb200.DistanceComparator(dm, N_Q, N_DB)
+    try:
+        slots = [(j, 0, 31, j) for j in range(N_Q)]
+        for p in range(3):
+            ce[p].query_upload_slots(data["qc"][p], slots)
+            me[p].query_upload_slots(data["qm"][p], slots)
+        exp = W.expected_bitmap(oracle, data["qc"], data["qm"], data["cs"], data["ms"], 16384)
+        ps = PlainScan(dm, ce, me, c, dc, N_Q, N_DB, 16384)
+        cands = ps.candidates()
+        assert {p for p, _, _ in cands} == {"split", "pair", "fused"}
+        for cand in cands:
+            ps.configure(cand)
+            dc.reset()
+            ps.scan()
+            dm.synchronize()
+            got = irisb200.bitmap_get(dc.fetch_bitmap(N_Q, N_DB), N_Q, N_DB)
+            assert np.array_equal(got, exp), f"candidate {cand}"
+        best = ps.tune()
+        assert best in cands and len(ps.tune_log) == len(cands)
+        ps.restore()
+    finally:
+        _close([dc, c] + ce + me)
