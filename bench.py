@@ -700,8 +700,8 @@ def run_ours(args):
             # the profile's launch covers `entries` DB entries; DRAM bytes grow in
             # proportion to the entries a launch scans (one query-plane re-read per
             # sweep of the SMs over the DB slabs), so scale to this launch
-            lg = pj.get("limb_gemm", {})
-            if lg.get("dram_bytes_per_launch") and lg.get("entries") and chosen[0] == "split":
+            lg = pj.get({"split": "limb_gemm", "pair": "limb_gemm_pair", "fused": "fused_scan"}[chosen[0]], {})
+            if lg.get("dram_bytes_per_launch") and lg.get("entries"):
                 traffic = lg["dram_bytes_per_launch"] * chunks[0][1] / lg["entries"]
         thr_avg = statistics.mean(thr_ms)
         mhz = clk_value.get("sm_mhz")
