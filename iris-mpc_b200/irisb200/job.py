@@ -204,6 +204,9 @@ def assemble_job_result(batch: BatchInfo, out: PassOutput, db_sizes, max_batch_s
                 if rid not in peers[i]:
                     peers[i].append(rid)
     filtered = [[x for x in ids if x <= U32_MAX - max_batch_size] for ids in match_ids]
+    for i in range(n):
+        if batch.request_types[i] == REAUTH and batch.request_ids[i] not in batch.reauth_target_indices:
+            raise ValueError(f"reauth request {batch.request_ids[i]!r} has no target index")
     reauth_ok = [batch.request_types[i] == REAUTH
                  and batch.reauth_target_indices[batch.request_ids[i]] in filtered[i] for i in range(n)]
     return ServerJobResult(

@@ -105,3 +105,11 @@ def test_pass_output_from_batched_results():
     r = assemble_job_result(batch, n, db_sizes=[100], max_batch_size=8)
     assert r.successful_reauths == [False, True, False]
     assert r.merged_results == [2, 9, 100] and r.matches == [True, True, False]
+
+
+def test_reauth_without_target_is_refused():
+    import pytest
+    batch = BatchInfo(["a"], ["reauth"])
+    out = _pass(final=[NON_MATCH_ID], counters=[0], lists=[[]])
+    with pytest.raises(ValueError, match="no target"):
+        assemble_job_result(batch, out, db_sizes=[10], max_batch_size=8)
