@@ -1039,7 +1039,6 @@ int irs_circuits_set_batch(irs_circuits* c, uint64_t batch_id) {
 
 static void base_params(irs_circuits* c, ThresholdParams& P) {
   memset(&P, 0, sizeof P);
-  P.one = 1;
   for (int p = 0; p < 3; p++) P.key[p] = c->keys[p];
   P.nonce = nonce_of(kDomCircuit, (uint32_t)c->dm->device);
   P.batch = c->batch;

@@ -92,14 +92,11 @@ struct WordRand {
 // memory, element i of this thread at pre[i * nt] (18 of them) and keystream
 // word (s, j) written to ks[(16 s + j) * nt].  Out of line for the same
 // instruction-cache reason as chacha12_x3.
-template <int FMA_ADDS>
-static __device__ __noinline__ void chacha12_x3_strided(const uint4* pre, uint32_t* ks, int nt, uint32_t ctr_lo,
-                                                        uint32_t one) {
+static __device__ __noinline__ void chacha12_x3_strided(const uint4* pre, uint32_t* ks, int nt, uint32_t ctr_lo) {
 #pragma unroll 1
   for (int s = 0; s < 3; s++) {
     const uint4* q = pre + 6 * s * nt;
-    chacha12_core_split<FMA_ADDS>(q[0], q[nt], q[2 * nt], q[3 * nt], q[4 * nt], q[5 * nt], ctr_lo, ks + 16 * s * nt,
-                                  nt, one);
+    chacha12_core(q[0], q[nt], q[2 * nt], q[3 * nt], q[4 * nt], q[5 * nt], ctr_lo, ks + 16 * s * nt, nt);
   }
 }
 
@@ -107,11 +104,7 @@ static __device__ __noinline__ void chacha12_x3_strided(const uint4* pre, uint32
 // of the thread's local memory: the block's threads interleave them
 // ([element][thread], so a warp's accesses hit consecutive words and never
 // conflict), `pre` and `ks` point at this thread's column and nt is the
-// thread count of the block.  Same keystream as WordRand.  FMA_ADDS of the
-// four additions of each ChaCha quarter round run on the FMA pipe as
-// multiply-adds by `one` (= 1, from the kernel parameters), which offloads the
-// ALU pipe that bounds the threshold kernels.
-template <int FMA_ADDS = 0>
+// thread count of the block.  Same keystream as WordRand.
 struct WordRandShared {
   ChaChaKey key[3];
   uint64_t nonce;
@@ -120,7 +113,6 @@ struct WordRandShared {
   uint4* pre;    // [18][nt] words-of-four: 6 per stream
   uint32_t* ks;  // [48][nt]: 16 per stream
   int nt;
-  uint32_t one = 1;
   __device__ void load(int b) {
     if (!prepared) {
       for (int s = 0; s < 3; s++) {
@@ -131,7 +123,7 @@ struct WordRandShared {
       }
       prepared = true;
     }
-    chacha12_x3_strided<FMA_ADDS>(pre, ks, nt, (uint32_t)(base + (uint64_t)b), one);
+    chacha12_x3_strided(pre, ks, nt, (uint32_t)(base + (uint64_t)b));
   }
   __device__ uint32_t k(int s, int j) const { return ks[(16 * s + j) * nt]; }
 };

@@ -139,59 +139,6 @@ IRS_HD void chacha12_core(uint4 k0, uint4 k1, uint4 cn, uint4 c1, uint4 c2, uint
   out[13 * stride] = x13 + cn.x; out[14 * stride] = x14 + cn.y; out[15 * stride] = x15 + cn.z;
 }
 
-#ifdef __CUDACC__
-// x * one + y as an integer multiply-add: with one = 1 it is x + y, issued to
-// the FMA pipe instead of the ALU pipe.  `one` must come from run-time data
-// (a kernel parameter) so that the compiler cannot turn it back into an add.
-__device__ __forceinline__ uint32_t mad_add(uint32_t x, uint32_t one, uint32_t y) {
-  uint32_t r;
-  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(one), "r"(y));
-  return r;
-}
-
-// ChaCha quarter round whose additions can run on the FMA pipe: FMA_ADDS = 0
-// (none, the plain quarter round), 2 (the two c += d) or 4 (all four).
-template <int FMA_ADDS>
-__device__ __forceinline__ void chacha_qr_split(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t one) {
-  a = FMA_ADDS >= 4 ? mad_add(b, one, a) : a + b; d ^= a; d = IRS_ROT16(d);
-  c = FMA_ADDS >= 2 ? mad_add(d, one, c) : c + d; b ^= c; b = rotl32(b, 12);
-  a = FMA_ADDS >= 4 ? mad_add(b, one, a) : a + b; d ^= a; d = IRS_ROT8(d);
-  c = FMA_ADDS >= 2 ? mad_add(d, one, c) : c + d; b ^= c; b = rotl32(b, 7);
-}
-
-// chacha12_core with chacha_qr_split<FMA_ADDS> quarter rounds (same keystream).
-template <int FMA_ADDS>
-__device__ __forceinline__ void chacha12_core_split(uint4 k0, uint4 k1, uint4 cn, uint4 c1, uint4 c2, uint4 c3,
-                                                    uint32_t ctr_lo, uint32_t* out, int stride, uint32_t one) {
-  const uint32_t s0 = 0x61707865u, s1 = 0x3320646eu, s2 = 0x79622d32u, s3 = 0x6b206574u;
-  uint32_t x0 = s0, x4 = k0.x, x8 = k1.x, x12 = ctr_lo;
-  chacha_qr_split<FMA_ADDS>(x0, x4, x8, x12, one);
-  uint32_t x1 = c1.x, x5 = c1.y, x9 = c1.z, x13 = c1.w;
-  uint32_t x2 = c2.x, x6 = c2.y, x10 = c2.z, x14 = c2.w;
-  uint32_t x3 = c3.x, x7 = c3.y, x11 = c3.z, x15 = c3.w;
-  chacha_qr_split<FMA_ADDS>(x0, x5, x10, x15, one);
-  chacha_qr_split<FMA_ADDS>(x1, x6, x11, x12, one);
-  chacha_qr_split<FMA_ADDS>(x2, x7, x8, x13, one);
-  chacha_qr_split<FMA_ADDS>(x3, x4, x9, x14, one);
-#pragma unroll
-  for (int i = 1; i < 6; i++) {
-    chacha_qr_split<FMA_ADDS>(x0, x4, x8, x12, one);
-    chacha_qr_split<FMA_ADDS>(x1, x5, x9, x13, one);
-    chacha_qr_split<FMA_ADDS>(x2, x6, x10, x14, one);
-    chacha_qr_split<FMA_ADDS>(x3, x7, x11, x15, one);
-    chacha_qr_split<FMA_ADDS>(x0, x5, x10, x15, one);
-    chacha_qr_split<FMA_ADDS>(x1, x6, x11, x12, one);
-    chacha_qr_split<FMA_ADDS>(x2, x7, x8, x13, one);
-    chacha_qr_split<FMA_ADDS>(x3, x4, x9, x14, one);
-  }
-  out[0 * stride] = x0 + s0; out[1 * stride] = x1 + s1; out[2 * stride] = x2 + s2; out[3 * stride] = x3 + s3;
-  out[4 * stride] = x4 + k0.x; out[5 * stride] = x5 + k0.y; out[6 * stride] = x6 + k0.z;
-  out[7 * stride] = x7 + k0.w; out[8 * stride] = x8 + k1.x; out[9 * stride] = x9 + k1.y;
-  out[10 * stride] = x10 + k1.z; out[11 * stride] = x11 + k1.w; out[12 * stride] = x12 + ctr_lo;
-  out[13 * stride] = x13 + cn.x; out[14 * stride] = x14 + cn.y; out[15 * stride] = x15 + cn.z;
-}
-#endif
-
 // chacha12_core from a contiguous prepared array pre[24] (16-byte aligned).
 IRS_HD void chacha12_block_prepared(const uint32_t* pre, uint32_t ctr_lo, uint32_t out[16]) {
   const uint4* q = reinterpret_cast<const uint4*>(pre);

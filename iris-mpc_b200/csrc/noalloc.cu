@@ -118,7 +118,6 @@ extern "C" int irs_circuits_compare_threshold_masked_many_noalloc(irs_circuits* 
   if (rc) return rc;
   if (n == 0) return IRS_OK;
   ThresholdParams P = {};
-  P.one = 1;
   for (int p = 0; p < 3; p++) {
     P.key[p] = v.keys[p];
     P.code[p] = code_a[p];

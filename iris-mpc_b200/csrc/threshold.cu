@@ -33,7 +33,6 @@ constexpr int kThreshThreads = 128;
 // Shared memory per thread of the keystream (WordRandShared): 18 prepared
 // words-of-four and 48 keystream words.
 constexpr int kRandSmemPerThread = 18 * 16 + 48 * 4;
-constexpr int kDefaultFmaAdds = 0;
 
 template <class WR>
 __device__ __forceinline__ void init_rand(WR& wr, const ThresholdParams& P, uint64_t word_id) {
@@ -44,21 +43,20 @@ __device__ __forceinline__ void init_rand(WR& wr, const ThresholdParams& P, uint
 }
 
 // This thread's keystream columns in the block's shared memory ([element][thread]).
-template <int THREADS, int FMA_ADDS>
-__device__ __forceinline__ void bind_rand(WordRandShared<FMA_ADDS>& wr, const ThresholdParams& P) {
+template <int THREADS>
+__device__ __forceinline__ void bind_rand(WordRandShared& wr) {
   extern __shared__ uint4 rand_smem[];
   wr.pre = rand_smem + threadIdx.x;
   wr.ks = reinterpret_cast<uint32_t*>(rand_smem + 18 * THREADS) + threadIdx.x;
   wr.nt = THREADS;
-  wr.one = P.one | 1u;  // 1, but run-time data
 }
 
-template <int STAGE, int FMA_ADDS>
+template <int STAGE>
 __global__ void __launch_bounds__(kThreshThreads) threshold_flat_kernel(const ThresholdParams P) {
   const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.n_words) return;
-  WordRandShared<FMA_ADDS> wr;
-  bind_rand<kThreshThreads>(wr, P);
+  WordRandShared wr;
+  bind_rand<kThreshThreads>(wr);
   init_rand(wr, P, P.word_base + w);
   const uint16_t* code[3] = {P.code[0] + 32 * w, P.code[1] + 32 * w, P.code[2] + 32 * w};
   const uint16_t* mask[3] = {P.mask[0] + 32 * w, P.mask[1] + 32 * w, P.mask[2] + 32 * w};
@@ -74,7 +72,7 @@ __global__ void __launch_bounds__(kThreshThreads) threshold_flat_kernel(const Th
 
 // The bitmap kernel indexes by global warp only, so its block size is free:
 // THREADS x MIN_BLOCKS sets the resident warps per SM the registers are sized for.
-template <int THREADS, int MIN_BLOCKS, int FMA_ADDS>
+template <int THREADS, int MIN_BLOCKS>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) threshold_bitmap_kernel(const ThresholdParams P) {
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t gwarp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -88,8 +86,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) threshold_bitmap_kernel(c
   const uint32_t m_read = valid ? m_local : (P.n_entries - 1);
   const uint64_t m_global = (uint64_t)P.m0 + m_local;
 
-  WordRandShared<FMA_ADDS> wr;
-  bind_rand<THREADS>(wr, P);
+  WordRandShared wr;
+  bind_rand<THREADS>(wr);
   init_rand(wr, P, ((uint64_t)P.m0 + m_read) * (uint64_t)(P.n_pad / 32) + slot);
   const size_t off = (size_t)m_read * P.n_pad + (size_t)slot * 32;
   uint32_t opened;
@@ -134,42 +132,16 @@ static cudaError_t allow_rand_smem(K kernel) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRandSmem);
 }
 
-// How many of the four additions of each ChaCha quarter round the threshold
-// kernels issue to the FMA pipe (0, 2 or 4); IRS_THRESHOLD_FMA_ADDS selects a
-// variant for tuning runs.
-static int fma_adds() {
-  static const int v = [] {
-    const char* e = getenv("IRS_THRESHOLD_FMA_ADDS");
-    const int x = e ? atoi(e) : kDefaultFmaAdds;
-    return (x == 0 || x == 2 || x == 4) ? x : kDefaultFmaAdds;
-  }();
-  return v;
-}
-
-template <int STAGE, int FMA_ADDS>
-static cudaError_t launch_flat_v(const ThresholdParams& P, unsigned grid, cudaStream_t stream) {
-  static cudaError_t attr = allow_rand_smem(threshold_flat_kernel<STAGE, FMA_ADDS>);
-  if (attr != cudaSuccess) return attr;
-  threshold_flat_kernel<STAGE, FMA_ADDS><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_threshold_flat(const ThresholdParams& P, int stage, cudaStream_t stream) {
   if (P.n_words == 0) return cudaSuccess;
-  const unsigned grid = (unsigned)((P.n_words + kThreshThreads - 1) / kThreshThreads);
-  if (stage != kStageFull) return launch_flat_v<kStageMsbOnly, kDefaultFmaAdds>(P, grid, stream);
-  switch (fma_adds()) {
-    case 2: return launch_flat_v<kStageFull, 2>(P, grid, stream);
-    case 4: return launch_flat_v<kStageFull, 4>(P, grid, stream);
-    default: return launch_flat_v<kStageFull, 0>(P, grid, stream);
-  }
-}
-
-template <int MIN_BLOCKS, int FMA_ADDS>
-static cudaError_t launch_bitmap_v(const ThresholdParams& P, unsigned grid, cudaStream_t stream) {
-  static cudaError_t attr = allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, MIN_BLOCKS, FMA_ADDS>);
+  static cudaError_t attr = [] {
+    cudaError_t e = allow_rand_smem(threshold_flat_kernel<kStageFull>);
+    return e == cudaSuccess ? allow_rand_smem(threshold_flat_kernel<kStageMsbOnly>) : e;
+  }();
   if (attr != cudaSuccess) return attr;
-  threshold_bitmap_kernel<kThreshThreads, MIN_BLOCKS, FMA_ADDS><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
+  const unsigned grid = (unsigned)((P.n_words + kThreshThreads - 1) / kThreshThreads);
+  if (stage == kStageFull) threshold_flat_kernel<kStageFull><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
+  else threshold_flat_kernel<kStageMsbOnly><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
   return cudaGetLastError();
 }
 
@@ -186,13 +158,15 @@ cudaError_t launch_threshold_bitmap(const ThresholdParams& P, cudaStream_t strea
     const char* e = getenv("IRS_THRESHOLD_WARPS_PER_SM");
     return e && atoi(e) == 8;
   }();
+  static cudaError_t attr = [] {
+    cudaError_t e = allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 2>);
+    return e == cudaSuccess ? allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 3>) : e;
+  }();
+  if (attr != cudaSuccess) return attr;
   const unsigned grid = (unsigned)((warps * 32 + kThreshThreads - 1) / kThreshThreads);
-  if (eight) return launch_bitmap_v<2, kDefaultFmaAdds>(P, grid, stream);
-  switch (fma_adds()) {
-    case 2: return launch_bitmap_v<3, 2>(P, grid, stream);
-    case 4: return launch_bitmap_v<3, 4>(P, grid, stream);
-    default: return launch_bitmap_v<3, 0>(P, grid, stream);
-  }
+  if (eight) threshold_bitmap_kernel<kThreshThreads, 2><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
+  else threshold_bitmap_kernel<kThreshThreads, 3><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_lift_flat(const ThresholdParams& P, uint16_t* corr, cudaStream_t stream) {

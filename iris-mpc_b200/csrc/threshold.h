@@ -14,7 +14,6 @@ struct ThresholdParams {
   uint64_t batch;
   const uint64_t* batch_dev;  // when set, the batch id is read from device memory
   uint32_t threshold_a;
-  uint32_t one;             // 1 (run-time data for the FMA-pipe additions of the keystream)
   // flat mode
   uint64_t n_words;
   uint64_t word_base;
