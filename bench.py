@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--serving-arms", default="served,plain", help="serving: which servers to run")
     ap.add_argument("--serving-rates-leg", default="300,600,1000",
                     help="default run: offered loads of its serving leg, requests/s (empty = skip)")
+    ap.add_argument("--serving-gemm", default="split", choices=["split", "pair"],
+                    help="serving: the DB engines' GEMM (pair = the two-SM kernel where the 256-row tile applies)")
+    ap.add_argument("--serving-leg-chunk", type=int, default=65536, help="default run: DB chunk per serving step")
     ap.add_argument("--serving-leg-seconds", type=float, default=5.0,
                     help="default run: seconds of Poisson arrivals per offered load of the serving leg")
     ap.add_argument("--latency-batches", type=int, default=200,
@@ -646,15 +649,16 @@ def run_ours(args):
         spl = {j: (int((j * 7919 + 13) % M), (j * 7) % 31 - 15) for j in range(0, nq_s, 10)}
         sqc, sqm = irisb200.synth_queries(DB_SEED + rank, Q_SEED + 2, nq_s, spl)
         app_c, app_m = append_records(ce, me, M)
-        srv = ContinuousServer(dm, ce, me, c, chunk=65536, row_capacity=q_cap, max_variants=min(q_cap // 2, 2048),
-                               max_reauth=64, threshold_a=A, seeds=seeds, db_capacity=M + 256)
+        srv = ContinuousServer(dm, ce, me, c, chunk=args.serving_leg_chunk, row_capacity=q_cap,
+                               max_variants=min(q_cap // 2, 2048), max_reauth=64, threshold_a=A, seeds=seeds,
+                               db_capacity=M + 256, gemm_pair=args.serving_gemm == "pair")
         warm = request_mix(40, sqc, sqm, spl, M, seed=99)
         srv.serve([0.0] * len(warm), warm)
         loads = []
         for li, lam in enumerate(rates):
             st = serve_load(srv, srv, lam, args.serving_leg_seconds, li, (sqc, sqm, spl, M, app_c, app_m), clk)
             st["vs_plain_value"] = st["comparisons_per_s"] / value
-            st["rows_x_entries_per_s"] = (st["mean_used_rows_per_step"] * 65536 /
+            st["rows_x_entries_per_s"] = (st["mean_used_rows_per_step"] * args.serving_leg_chunk /
                                           (st["mean_step_interval_ms"] * 1e-3))
             loads.append(st)
         under = [x for x in loads if x["p99_ms"] < 1000.0]
@@ -667,7 +671,7 @@ def run_ours(args):
             "config": {"workload": "continuous serving: Poisson arrivals, 80% uniqueness / 20% reauth, 1% appends, "
                                    f"rotations 1/16/31, 50% mirrored, {args.serving_leg_seconds:g} s of arrivals per "
                                    "offered load",
-                       "row_capacity": q_cap, "chunk": 65536,
+                       "row_capacity": q_cap, "chunk": args.serving_leg_chunk, "gemm": args.serving_gemm,
                        "saturation": "the highest completed requests/s over the offered loads (a request counts "
                                      "from its arrival to its completion; the rate runs to the last completion)"},
         }
@@ -925,7 +929,7 @@ def run_serving(args):
     app_c, app_m = append_records(ce, me, M)
     max_var = min(R // 2, 4096)
     srv = ContinuousServer(dm, ce, me, c, chunk=chunk, row_capacity=R, max_variants=max_var, max_reauth=64,
-                           threshold_a=A, seeds=seeds, db_capacity=cap)
+                           threshold_a=A, seeds=seeds, db_capacity=cap, gemm_pair=args.serving_gemm == "pair")
     plain = PlainBatchServer(dm, ce, me, c, chunk=chunk, max_slots=64, threshold_a=A, db_capacity=cap)
     # warm both paths (kernels, graphs of nothing, allocator pools)
     warm = request_mix(40, qc, qm, planted, M, seed=99)
@@ -959,6 +963,7 @@ def run_serving(args):
         "config": {"workload": f"serving: Poisson arrivals, {M} share-DB entries per party resident, 80% uniqueness "
                                "/ 20% reauth, 1% appends, rotations 1/16/31, 50% mirrored",
                    "row_capacity": R, "row_capacity_planned_from_free_hbm": R_plan, "chunk": chunk,
+                   "gemm": args.serving_gemm,
                    "max_variants": max_var, "threshold_a": A, "serve_seconds": args.serve_seconds,
                    "value_rule": "highest comparisons/s over the offered loads whose p99 latency is below 1 s",
                    "comparison": "one (query orientation, DB entry) pair; a reauth orientation is one comparison",

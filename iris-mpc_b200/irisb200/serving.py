@@ -114,11 +114,15 @@ class ContinuousServer:
 
     def __init__(self, dm, code_engines, mask_engines, circuits, chunk: int = 65536, row_capacity: int = 2048,
                  max_variants: int = 512, max_reauth: int = 64, threshold_a: int = 16384, seeds=None,
-                 db_capacity: int | None = None):
+                 db_capacity: int | None = None, gemm_pair: bool = False):
         if max_variants + 2 > row_capacity:
             raise ValueError("row_capacity must exceed max_variants (base pool and row table share the staging)")
         self.dm = dm
         self.ce, self.me = list(code_engines), list(mask_engines)
+        # the DB engines' GEMM: the two-SM kernel where the 256-row tile applies
+        # (irs_sharedb_set_pair); close() restores the default
+        for e in self.ce + self.me:
+            e.set_pair(gemm_pair)
         self.c = circuits
         self.A = threshold_a
         self.chunk = max(32, chunk // 32 * 32)
@@ -547,6 +551,9 @@ class ContinuousServer:
             e.set_db_len(self.db_len)
 
     def close(self) -> None:
+        self.dm.synchronize()
+        for e in self.ce + self.me:
+            e.set_pair(False)
         for o in self.sce + self.sme + [self.dc, self.sdc]:
             o.close()
         for e in self.events:
