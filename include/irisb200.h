@@ -409,8 +409,10 @@ int irs_dc_compare_threshold_open_prepared(irs_distance_comparator* dc, irs_circ
  * two-launch path's bit for bit.  Needs the padded query rows in multiples of
  * 128.  The first call allocates the comparator's ring (n_SMs x 196,608
  * bytes; a call with len = 0 only allocates), so make it before any graph
- * capture; later calls are graph-capturable.  Afterwards the engines hold no
- * dot shares (irs_sharedb_fetch_results refuses). */
+ * capture; later calls are graph-capturable.  The ring belongs to the
+ * comparator: two scans of one comparator must not overlap on the GPU (issue
+ * them on one stream, as all of a comparator's calls).  Afterwards the
+ * engines hold no dot shares (irs_sharedb_fetch_results refuses). */
 int irs_dc_scan_fused(irs_distance_comparator* dc, irs_circuits* c, irs_sharedb* const code_engines[3],
                       irs_sharedb* const mask_engines[3], size_t offset, size_t len, size_t n_slots,
                       uint32_t threshold_a, int use_segments, void* stream);
