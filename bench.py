@@ -84,9 +84,9 @@ def parse():
     ap.add_argument("--serving-arms", default="served,plain", help="serving: which servers to run")
     ap.add_argument("--serving-rates-leg", default="300,600,1000",
                     help="default run: offered loads of its serving leg, requests/s (empty = skip)")
-    ap.add_argument("--serving-gemm", default="split", choices=["split", "pair"],
+    ap.add_argument("--serving-gemm", default="pair", choices=["split", "pair"],
                     help="serving: the DB engines' GEMM (pair = the two-SM kernel where the 256-row tile applies)")
-    ap.add_argument("--serving-leg-chunk", type=int, default=65536, help="default run: DB chunk per serving step")
+    ap.add_argument("--serving-leg-chunk", type=int, default=32768, help="default run: DB chunk per serving step")
     ap.add_argument("--serving-leg-seconds", type=float, default=5.0,
                     help="default run: seconds of Poisson arrivals per offered load of the serving leg")
     ap.add_argument("--latency-batches", type=int, default=200,
