@@ -124,3 +124,44 @@ def test_serving_alone_equals_mix_and_cpu(oracle, world):
     assert state["db_len"] == N_DB + 1 and state["batch_counter"] >= srv.steps
     srv.restore(state)
     assert srv.dm.batch_counter() == state["batch_counter"] and srv.db_len == N_DB + 1
+
+
+def test_two_sm_gemm_server_equals_default(dm, oracle, world):
+    """With the two-SM GEMM (gemm_pair=True; it applies once the rows in flight
+    pad to the 256-row tile: here 30 variants of 31 rotations, 1024 rows) the
+    server returns the same matches as with the default GEMM, and the CPU
+    path's."""
+    cs, ms = world["cs"][:, :N_DB], world["ms"][:, :N_DB]
+    rows = 1024
+    ce = [irisb200.ShareDB(p, dm, CHUNK, rows, 12800, W.SEEDS[p]) for p in range(3)]
+    me = [irisb200.ShareDB(p, dm, CHUNK, rows, 6400, W.SEEDS[p]) for p in range(3)]
+    c = irisb200.Circuits(dm, W.SEEDS)
+    try:
+        for p in range(3):
+            ce[p].alloc_db(N_DB)
+            me[p].alloc_db(N_DB)
+            ce[p].load_records(0, cs[p])
+            me[p].load_records(0, ms[p])
+        reqs = [Request(code=world["qc"][:, j % 5], mask=world["qm"][:, j % 5], n_rot=31, mirrored=j % 2 == 1)
+                for j in range(20)]
+        got = {}
+        for pair in (False, True):
+            srv = ContinuousServer(dm, ce, me, c, chunk=CHUNK, row_capacity=rows, max_variants=32, max_reauth=4,
+                                   threshold_a=A, db_capacity=N_DB, gemm_pair=pair)
+            try:
+                comps = srv.serve([0.0] * len(reqs), reqs)
+                assert srv.stats["rows"] >= 1024 * srv.stats["steps"] * 0.5, "the 256-row tile was not reached"
+            finally:
+                srv.close()
+            got[pair] = {cp.idx: (cp.result.matches, cp.result.mirror_matches) for cp in comps}
+        assert got[True] == got[False]
+        for j in range(5):
+            for mir in (False, True):
+                exp = W.expected_variant_hits(oracle, cs, ms, world["qc"][:, j], world["qm"][:, j], list(range(31)),
+                                              mir, np.arange(N_DB), A)
+                i = j if (not mir or j % 2 == 1) else j + 5  # odd requests carry a mirrored variant
+                assert got[True][i][1 if mir else 0] == exp[:256], f"query {j} mirrored={mir}"
+    finally:
+        c.close()
+        for e in ce + me:
+            e.close()
