@@ -730,8 +730,9 @@ def run_ours(args):
                        "l2": "no flush: inputs (60.4 GB share DB) exceed the 126 MB L2",
                        "parallelism": f"db-shard x{world}, 3 co-resident parties per GPU",
                        "db_chunk": chunks[0][1], "db_pass_path": chosen[0],
-                       "db_pass_choice": ("PlainScan.tune on the batch: "
-                                          + "; ".join(f"{p}/{t}/{ch}: {ms:.1f} ms" for (p, t, ch), ms in ps.tune_log))
+                       "db_pass_choice": ("PlainScan.tune on the batch, ms per pass (first round, then the "
+                                          "finalists' means over the interleaved rounds): "
+                                          + "; ".join(f"{p}/{t}/{ch}: {ms:.1f}" for (p, t, ch), ms in ps.tune_log))
                                          if ps.tune_log else "fixed (--plain-path)"},
             "latency_ms": {"p50": pct(batch_ms, 50), "p99": pct(batch_ms, 99), "of": f"the {args.steps} timed steps",
                            "e2e_p50": pct(lat, 50), "e2e_p99": pct(lat, 99)},

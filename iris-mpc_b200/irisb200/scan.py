@@ -50,7 +50,7 @@ class PlainScan:
         ch = self.cand[2]
         return [(o, min(ch, self.db_len - o)) for o in range(0, self.db_len, ch)]
 
-    def scan(self, events=None, stream_events=None) -> None:
+    def scan(self, events=None) -> None:
         """One pass over the DB (no comparator reset).  events: optional list,
         per chunk, of three callables recorded before the chunk, between its
         two launches (split / pair) and after it."""
@@ -70,26 +70,45 @@ class PlainScan:
             if events:
                 events[k][2]()
 
-    def tune(self, cands=None, passes: int = 2):
-        """Times `passes` consecutive passes of each candidate after a warm
-        pass (the power-capped clock settles differently for each path) and
-        keeps the fastest; returns it."""
-        best, best_t = None, float("inf")
-        self.tune_log = []
-        for cand in cands or self.candidates():
-            self.configure(cand)
+    def _time(self, cand, passes: int) -> float:
+        """Seconds per pass of `passes` consecutive passes after a warm one."""
+        self.configure(cand)
+        self.dc.reset()
+        self.scan()
+        self.dm.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(passes):
             self.dc.reset()
             self.scan()
-            self.dm.synchronize()
-            t0 = time.perf_counter()
-            for _ in range(passes):
-                self.dc.reset()
-                self.scan()
-            self.dm.synchronize()
-            el = (time.perf_counter() - t0) / passes
+        self.dm.synchronize()
+        return (time.perf_counter() - t0) / passes
+
+    def tune(self, cands=None, passes: int = 2, finalists: int = 3, rounds: int = 2):
+        """Times `passes` consecutive passes of each candidate after a warm
+        pass (the power-capped clock settles differently for each path), then
+        re-times the `finalists` fastest interleaved for `rounds` rounds (the
+        clock drifts over a tuning run, and candidates timed far apart are not
+        comparable at the 2% level) and keeps the best mean of those rounds;
+        returns it.  tune_log: (candidate, ms per pass) of the first round,
+        then (candidate, mean ms over the interleaved rounds) per finalist."""
+        self.tune_log = []
+        first = []
+        for cand in cands or self.candidates():
+            el = self._time(cand, passes)
+            first.append((el, cand))
             self.tune_log.append((cand, el * 1e3))
-            if el < best_t:
-                best, best_t = cand, el
+        first.sort(key=lambda x: x[0])
+        top = [c for _, c in first[:max(1, finalists)]]
+        if len(top) > 1 and rounds > 0:
+            acc = {c: 0.0 for c in top}
+            for _ in range(rounds):
+                for c in top:
+                    acc[c] += self._time(c, passes)
+            means = {c: acc[c] / rounds for c in top}
+            self.tune_log += [(c, means[c] * 1e3) for c in top]
+            best = min(top, key=lambda c: means[c])
+        else:
+            best = top[0]
         self.configure(best)
         return best
 
