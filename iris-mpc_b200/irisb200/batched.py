@@ -16,7 +16,8 @@ The device work of a batch -- comparator reset, the six limb GEMMs and the
 fused threshold/open/OR per DB chunk, the result merge -- is captured once per
 layout into a CUDA graph and replayed; the ChaCha batch id comes from the
 device batch counter, so a replay draws fresh randomness.  The autotuner picks,
-per padded row count, by timing each candidate's captured pass once: the path
+per padded row count, by timing each candidate's captured pass (and the three
+fastest again, interleaved, against the clock's drift): the path
 (the GEMM launch then the threshold launch per chunk, the same with the two-SM
 GEMM, or the one-kernel fused GEMM + threshold scan), the GEMM's tile width
 along the query rows and the DB chunk length.
