@@ -638,6 +638,11 @@ int gemm_block_n_for(uint32_t n_pad) {
 // bandwidth under this tensor-bound kernel, and keeping the queries with
 // evict_last saved 2% of the traffic while slowing the GEMM by 3% and the
 // following threshold kernel by 18% (the pinned lines outlive the GEMM).
+// Marking the streaming DB evict_first (value 2) instead tripled the reads
+// on 65,536-entry chunks (31-48 GB against 13.7 GB per launch: each DB tile
+// is read by the wave's 8 query-tile CTAs, and the hint drops it between
+// them), and under the power cap the clock fell from 1567 to ~1365 MHz, 14%
+// slower per batch.
 static uint32_t gemm_l2_hint() {
   static const uint32_t hint = [] {
     const char* e = getenv("IRS_GEMM_L2HINT");
