@@ -4,9 +4,11 @@
 Workload (the GPU plain drop-in configuration): 3 parties co-resident on one
 GPU, 64 queries x 31 rotations (1984 query rows in 64 slots of 32) against
 524,288 share-DB entries per party, threshold ratio 0.375 (A = 16384).  One
-step = one batch, the DB scanned in chunks of 65,536 entries (--db-chunk): per
-chunk the six limb GEMMs (3 parties x code/mask) in one tcgen05 launch, then
-the fused threshold + open + rotation OR into the match bitmap.
+step = one batch, the DB scanned in chunks: per chunk the six limb GEMMs (3
+parties x code/mask) in one tcgen05 launch, then the fused threshold + open +
+rotation OR into the match bitmap.  The chunk length and the GEMM variant
+(one-SM, two-SM, or the one-kernel fused scan) are picked on the batch by
+irisb200.scan.PlainScan.tune, or fixed with --plain-path / --db-chunk.
 One comparison = one (query iris, DB entry) pair over all 31 rotations,
 computed jointly by the three parties.
 
@@ -21,8 +23,12 @@ Further legs of the default run, on the same engines and DB (rank 0 of a
 CUDA events), `batched` (100 batches of 256 uneven requests through
 BatchedEngine), `serving` (ContinuousServer at 300 / 600 / 1000 requests/s,
 5 s of Poisson arrivals each), the cuBLAS limb GEMMs of the reference on the
-same shapes, and `sweep` (the GEMM and comparison roofline sweep, each row
-timed for at least a second with its own clock record).  `roofline` is the
+same shapes, `fused_scan` (the plain batch on the one-kernel fused scan),
+and `sweep` (the GEMM and comparison roofline sweep, each row timed for at
+least a second with its own clock record).  `cpu_baseline` times the CPU
+restatement of the reference's CPU path, `cpu_mpc_simulation` the whole
+3-party protocol of the path on the CPU (masked dot shares, threshold
+circuit, open, rotation OR), both on bounded samples.  `roofline` is the
 limb GEMM's, `roofline_threshold` the threshold kernel's (instruction issue),
 `cycles_per_batch` the GEMM's and cuBLAS's device time x sampled SM clock.
 
@@ -200,17 +206,30 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+_CPU_SAMPLES = {}
+
+
+def _cpu_sample(n_query: int, n_db: int):
+    """The seeded CPU sample (oracle module, workload module, DB and query
+    shares, rotated query rows), built once per shape."""
+    key = (n_query, n_db)
+    if key not in _CPU_SAMPLES:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle import oracle as O
+        import workload as W
+        O.build()
+        codes, masks, cs, ms = W.make_db(O, n_db, DB_SEED)
+        planted = {j: (int(j * 997 % n_db), (j % 31) - 15) for j in range(0, n_query, 10)}
+        qc, qm, _ = W.make_queries(O, n_query, codes, masks, Q_SEED, planted)
+        q_code = [W.rotated_rows(O, qc[p]) for p in range(3)]
+        q_mask = [W.rotated_rows(O, qm[p]) for p in range(3)]
+        _CPU_SAMPLES[key] = (O, W, cs, ms, q_code, q_mask)
+    return _CPU_SAMPLES[key]
+
+
 def cpu_baseline(n_query=8, n_db=8192, min_seconds=10.0):
     """The CPU restatement of the reference's CPU path on config 0's shape."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle import oracle as O
-    import workload as W
-    O.build()
-    codes, masks, cs, ms = W.make_db(O, n_db, DB_SEED)
-    planted = {j: (int(j * 997 % n_db), (j % 31) - 15) for j in range(0, n_query, 10)}
-    qc, qm, _ = W.make_queries(O, n_query, codes, masks, Q_SEED, planted)
-    q_code = [W.rotated_rows(O, qc[p]) for p in range(3)]
-    q_mask = [W.rotated_rows(O, qm[p]) for p in range(3)]
+    O, W, cs, ms, q_code, q_mask = _cpu_sample(n_query, n_db)
     cores = os.cpu_count() or 1
     reps, t0 = 0, time.perf_counter()
     while True:
@@ -223,6 +242,57 @@ def cpu_baseline(n_query=8, n_db=8192, min_seconds=10.0):
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{n_query} queries x 31 rotations vs {n_db} entries, 3 parties, {reps} pass(es), "
                       f"{el:.1f} s, OpenMP on {cores} threads"}
+
+
+def cpu_mpc_simulation(n_query=8, n_db=8192, n_entries=1024, min_seconds=10.0):
+    """The full 3-party protocol of the path simulated on the CPU (a secondary
+    CPU number beside cpu_baseline): per party the u16 dot shares of 32-row
+    query slots (31 rotations + one zero row) against the party's DB shares
+    with its zero-share mask (share_db.rs:815-821), the threshold circuit
+    with its ChaCha12 randomness (protocol.rs:2519-2546), the open and the OR
+    over each slot's 31 rotations; on the first `n_entries` entries of the
+    cpu_baseline sample, checked against the plaintext predicate there."""
+    import numpy as np
+    O, W, cs, ms, q_code, q_mask = _cpu_sample(n_query, n_db)
+    q_pad = 32 * n_query
+
+    def slots(rows):
+        out = np.zeros((q_pad, rows.shape[1]), np.uint16)
+        for j in range(n_query):
+            out[32 * j:32 * j + 31] = rows[31 * j:31 * j + 31]
+        return out
+
+    qs_code = [slots(q_code[p]) for p in range(3)]
+    qs_mask = [slots(q_mask[p]) for p in range(3)]
+    db_code = [np.ascontiguousarray(cs[p][:n_entries]) for p in range(3)]
+    db_mask = [np.ascontiguousarray(ms[p][:n_entries]) for p in range(3)]
+    keys = [W.SEEDS[p][0] for p in range(3)]
+
+    def one_pass(batch):
+        code_parts, mask_parts = [], []
+        for p in range(3):
+            own, prev = W.SEEDS[p]
+            d = O.dot_u16(qs_code[p], db_code[p]).T
+            code_parts.append(O.mask_dot_shares(d, 0, q_pad, 1, own, prev, O.DOM_CODE_DOT, 0, batch).reshape(-1))
+            d = O.dot_u16(qs_mask[p], db_mask[p]).T
+            mask_parts.append(O.mask_dot_shares(d, 0, q_pad, 2, own, prev, O.DOM_MASK_DOT, 0, batch).reshape(-1))
+        rev = O.threshold_words(code_parts, mask_parts, 16384, keys, dev=0, batch=batch)["revealed"]
+        return (rev.reshape(n_entries, n_query) & np.uint32(0x7FFFFFFF)).T != 0
+
+    cores = os.cpu_count() or 1
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        got = one_pass(reps)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= 50:
+            break
+    expect = O.cpu_plain_match(q_code, q_mask, n_query, db_code, db_mask, 16384, cores).astype(bool)
+    return {"value": reps * n_query * n_entries / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "equal_to_plaintext": bool(np.array_equal(got, expect)), "matches": int(got.sum()),
+            "sample": f"{n_query} queries x 31 rotations (32-row slots) vs {n_entries} entries, 3 parties: "
+                      f"masked dot shares, threshold circuit, open, rotation OR; {reps} pass(es), {el:.1f} s, "
+                      f"OpenMP on {cores} threads"}
 
 
 def pct(values, q: float) -> float:
@@ -795,6 +865,7 @@ def run_ours(args):
             rf["peak_source"] = "fallback: 2 x 1.4 PFLOP/s bf16 sustained (MEASURED_PEAKS.json absent)"
         if world == 1 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline()
+            result["cpu_mpc_simulation"] = cpu_mpc_simulation()
         print(json.dumps(result), flush=True)
 
     dm.close()

@@ -85,3 +85,13 @@ def test_percentiles_and_threshold_roofline(tmp_path, monkeypatch):
     rf = bench.threshold_roofline(10.0, 1000, 148, 1500.0, [(0, 1)])
     assert abs(rf["achieved"] - 20000.0 * 1000 / 0.01) < 1e-3
     assert abs(rf["frac"] - rf["achieved"] / rf["peak"]) < 1e-12
+
+
+def test_cpu_mpc_simulation_matches_plaintext():
+    """The secondary CPU leg runs the whole 3-party protocol (masked dot
+    shares, threshold circuit, open, rotation OR) on the oracle and must equal
+    the plaintext predicate on its sample; query 0 is planted at entry 0."""
+    out = bench.cpu_mpc_simulation(n_query=2, n_db=48, n_entries=40, min_seconds=0.0)
+    assert out["equal_to_plaintext"]
+    assert out["matches"] >= 1
+    assert out["value"] > 0 and out["kind"] == "port"
