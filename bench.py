@@ -86,7 +86,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serving: arrival window per load")
     ap.add_argument("--chunk", type=int, default=65536, help="serving: DB chunk per step")
     ap.add_argument("--db-chunk", type=int, default=65536,
-                    help="plain step: DB entries per GEMM + threshold launch pair (0 = whole DB per launch)")
+                    help="plain step with a fixed --plain-path: DB entries per launch pair (0 = whole DB "
+                         "per launch); the tuned path picks its own")
     ap.add_argument("--serving-arms", default="served,plain", help="serving: which servers to run")
     ap.add_argument("--serving-rates-leg", default="300,600,1000",
                     help="default run: offered loads of its serving leg, requests/s (empty = skip)")
@@ -597,8 +598,9 @@ def run_ours(args):
         latency.update(warmup=args.latency_warmup, clocks=clk.summary(clk.windows[-1]),
                        comparisons_per_s=comps * len(lat_b) / (sum(lat_b) * 1e-3),
                        rows_x_entries_per_s=NQ * 31 * M * len(lat_b) / (sum(lat_b) * 1e-3),
-                       timing="device time of each plain batch (comparator reset, 8 chunk pairs of GEMM + "
-                              "threshold/open/OR), CUDA events on the launching stream, batches back to back "
+                       timing="device time of each plain batch (comparator reset, one GEMM + threshold/open/OR "
+                              "launch pair per DB chunk of the chosen path, or one fused launch per chunk), CUDA "
+                              "events on the launching stream, batches back to back "
                               "after the warm-up; queries resident")
 
     # ---------------- end-to-end timing through the public API ----------------
