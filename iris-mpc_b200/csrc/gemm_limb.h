@@ -47,6 +47,10 @@ struct GemmParams {
   // Test hook: CTA 0 issues no TMA loads, so its MMA's first stage wait runs
   // out (kErrTimeoutFull) and the kernel returns with the error word set.
   uint32_t test_stall;
+  // Serpentine K order: a CTA walks K backwards on its odd tile iterations,
+  // so the query K blocks the previous wave of CTAs loaded last are the first
+  // this wave needs.  Integer accumulation: the result does not depend on it.
+  uint32_t serpentine;
 };
 
 // Builds a 2-D u8 tensor map (inner dim K, outer dim rows) with 128x`box_rows`
