@@ -286,7 +286,7 @@ def cpu_mpc_simulation(n_query=8, n_db=8192, n_entries=1024, min_seconds=10.0):
         got = one_pass(reps)
         reps += 1
         el = time.perf_counter() - t0
-        if el >= min_seconds or reps >= 50:
+        if el >= min_seconds or reps >= 200:
             break
     expect = O.cpu_plain_match(q_code, q_mask, n_query, db_code, db_mask, 16384, cores).astype(bool)
     return {"value": reps * n_query * n_entries / el, "unit": UNIT, "cores": cores, "kind": "port",
