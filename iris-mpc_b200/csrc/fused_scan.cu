@@ -39,6 +39,7 @@
 #include "fused_scan.h"
 #include "gemm_limb.h"
 #include "tc_sm100.cuh"
+#include "launch_attr.cuh"
 #include "threshold.h"
 #include "threshold_emit.cuh"
 
@@ -320,12 +321,9 @@ __global__ void __launch_bounds__(kFThreads, 1) fused_scan_kernel(const __grid_c
 int fused_scan_grid(const FusedParams& F, int n_sms) { return F.total_work < n_sms ? F.total_work : n_sms; }
 
 cudaError_t launch_fused_scan(FusedParams& F, int n_sms, cudaStream_t stream) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(fused_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem);
-    if (e != cudaSuccess) return e;
-    attr_done = true;
-  }
+  static std::atomic<uint64_t> attr_done{0};
+  cudaError_t e = smem_limit_once(fused_scan_kernel, kFSmem, attr_done);
+  if (e != cudaSuccess) return e;
   if (F.wait_timeout_ns == 0) F.wait_timeout_ns = kGemmWaitTimeoutNs;
   const int grid = fused_scan_grid(F, n_sms);
   if (grid <= 0) return cudaSuccess;

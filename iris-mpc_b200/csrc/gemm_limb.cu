@@ -30,6 +30,7 @@
 #include "common.cuh"
 #include "gemm_limb.h"
 #include "tc_sm100.cuh"
+#include "launch_attr.cuh"
 
 namespace irs {
 
@@ -589,13 +590,9 @@ int make_tmap_u8(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k, 
 template <int BN>
 static cudaError_t launch_bn(const GemmParams& P, int n_sms, cudaStream_t stream) {
   using C = Cfg<BN>;
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(limb_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         C::kSmemBytes);
-    if (e != cudaSuccess) return e;
-    attr_done = true;
-  }
+  static std::atomic<uint64_t> attr_done{0};
+  cudaError_t e = smem_limit_once(limb_gemm_kernel<BN>, C::kSmemBytes, attr_done);
+  if (e != cudaSuccess) return e;
   const int grid = P.total_tiles < n_sms ? P.total_tiles : n_sms;
   if (grid <= 0) return cudaSuccess;
   limb_gemm_kernel<BN><<<grid, kThreads, C::kSmemBytes, stream>>>(P);
@@ -603,13 +600,9 @@ static cudaError_t launch_bn(const GemmParams& P, int n_sms, cudaStream_t stream
 }
 
 static cudaError_t launch_pair(const GemmParams& P, int n_sms, cudaStream_t stream) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(limb_gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Cfg2::kSmemBytes);
-    if (e != cudaSuccess) return e;
-    attr_done = true;
-  }
+  static std::atomic<uint64_t> attr_done{0};
+  cudaError_t e = smem_limit_once(limb_gemm_pair_kernel, Cfg2::kSmemBytes, attr_done);
+  if (e != cudaSuccess) return e;
   const int clusters = P.total_tiles < n_sms / 2 ? P.total_tiles : n_sms / 2;
   if (clusters <= 0) return cudaSuccess;
   limb_gemm_pair_kernel<<<2 * clusters, kThreads, Cfg2::kSmemBytes, stream>>>(P);

@@ -24,6 +24,7 @@
 #include "circuit.cuh"
 #include "threshold.h"
 #include "threshold_emit.cuh"
+#include "launch_attr.cuh"
 
 namespace irs {
 
@@ -128,16 +129,15 @@ __global__ void __launch_bounds__(kThreshThreads) lift_flat_kernel(const Thresho
 constexpr int kRandSmem = kThreshThreads * kRandSmemPerThread;  // 61,440 bytes per block
 
 template <class K>
-static cudaError_t allow_rand_smem(K kernel) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kRandSmem);
+static cudaError_t allow_rand_smem(K kernel, std::atomic<uint64_t>& done) {
+  return smem_limit_once(kernel, kRandSmem, done);
 }
 
 cudaError_t launch_threshold_flat(const ThresholdParams& P, int stage, cudaStream_t stream) {
   if (P.n_words == 0) return cudaSuccess;
-  static cudaError_t attr = [] {
-    cudaError_t e = allow_rand_smem(threshold_flat_kernel<kStageFull>);
-    return e == cudaSuccess ? allow_rand_smem(threshold_flat_kernel<kStageMsbOnly>) : e;
-  }();
+  static std::atomic<uint64_t> done_full{0}, done_msb{0};
+  cudaError_t attr = allow_rand_smem(threshold_flat_kernel<kStageFull>, done_full);
+  if (attr == cudaSuccess) attr = allow_rand_smem(threshold_flat_kernel<kStageMsbOnly>, done_msb);
   if (attr != cudaSuccess) return attr;
   const unsigned grid = (unsigned)((P.n_words + kThreshThreads - 1) / kThreshThreads);
   if (stage == kStageFull) threshold_flat_kernel<kStageFull><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
@@ -158,10 +158,9 @@ cudaError_t launch_threshold_bitmap(const ThresholdParams& P, cudaStream_t strea
     const char* e = getenv("IRS_THRESHOLD_WARPS_PER_SM");
     return e && atoi(e) == 8;
   }();
-  static cudaError_t attr = [] {
-    cudaError_t e = allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 2>);
-    return e == cudaSuccess ? allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 3>) : e;
-  }();
+  static std::atomic<uint64_t> done_8{0}, done_12{0};
+  cudaError_t attr = eight ? allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 2>, done_8)
+                           : allow_rand_smem(threshold_bitmap_kernel<kThreshThreads, 3>, done_12);
   if (attr != cudaSuccess) return attr;
   const unsigned grid = (unsigned)((warps * 32 + kThreshThreads - 1) / kThreshThreads);
   if (eight) threshold_bitmap_kernel<kThreshThreads, 2><<<grid, kThreshThreads, kRandSmem, stream>>>(P);
