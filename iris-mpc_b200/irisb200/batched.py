@@ -237,16 +237,22 @@ class BatchedEngine:
         threshold launch per chunk; "pair": the same with the two-SM GEMM on
         the 256-row tile; "fused": the one-kernel GEMM + threshold scan
         (128-row tiles).  The 64-row GEMM tile is a candidate up to 768 rows,
-        where the pass is close to streaming the DB."""
+        where the pass is close to streaming the DB.  Chunks of 131,072 down to
+        8,192 entries: under the power cap, shorter GEMM + threshold
+        alternations keep the SM clock higher (two-SM GEMM on a 524,288-entry
+        plain batch: 163.7 ms per batch at 32,768-entry chunks, 157-161 at
+        16,384, 154-156 at 8,192 on one GPU), while very short launches lose
+        their last partial wave; the fused kernel is timed on the three
+        longest."""
         n_pad = (n_rows + 63) // 64 * 64
         full = (db_len + 31) // 32 * 32
-        chunks = sorted({min(full, c) for c in (131072, 65536, 32768)}, reverse=True)
+        chunks = sorted({min(full, c) for c in (131072, 65536, 32768, 16384, 8192)}, reverse=True)
         tiles = [t for t in (256, 128, 64) if n_pad % t == 0 and (t != 64 or n_pad <= 768)] or [64]
         out = [("split", t, ch) for t in tiles for ch in chunks]
         if n_pad % 256 == 0:
             out += [("pair", 256, ch) for ch in chunks]
         if n_pad % 128 == 0:
-            out += [("fused", 128, ch) for ch in chunks]
+            out += [("fused", 128, ch) for ch in chunks[:3]]
         return out
 
     def _configure(self, path: str, tile: int) -> None:

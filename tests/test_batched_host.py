@@ -196,14 +196,15 @@ def test_autotuner_candidates():
     """The tuner's candidates: the two-launch path at every tile width that
     divides the padded rows (the 64-row tile only up to 768 rows), the two-SM
     GEMM where the 256-row tile applies, the fused scan where the rows are a
-    multiple of 128, each at 131,072 / 65,536 / 32,768-entry chunks (capped at
-    the DB)."""
+    multiple of 128; the two-launch paths at 131,072 down to 8,192-entry
+    chunks, the fused scan at the three longest (all capped at the DB)."""
     from irisb200.batched import BatchedEngine
     c = BatchedEngine._candidates(2048, 524288)
     assert ("split", 256, 131072) in c and ("split", 128, 32768) in c
     assert not any(t == 64 for _, t, _ in c)
     assert ("pair", 256, 65536) in c and ("fused", 128, 32768) in c
-    assert len(c) == 2 * 3 + 3 + 3
+    assert ("pair", 256, 8192) in c and ("split", 256, 16384) in c and ("fused", 128, 16384) not in c
+    assert len(c) == 2 * 5 + 5 + 3
     c = BatchedEngine._candidates(640, 524288)
     assert {t for p, t, _ in c if p == "split"} == {128, 64}
     assert not any(p == "pair" for p, _, _ in c) and any(p == "fused" for p, _, _ in c)
