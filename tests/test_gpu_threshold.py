@@ -45,7 +45,10 @@ def _u32_words(u64_words):
     return np.ascontiguousarray(u64_words).view(np.uint32)
 
 
-@pytest.mark.parametrize("n,threshold_a", [(64 * 1024, 20316), (64 * 4096, 16384), (64, 20316)])
+# 12,507,136 = INPUTS_PER_GPU_SIZE of iris-mpc-gpu/tests/threshold.rs:24, the
+# reference test's own size.
+@pytest.mark.parametrize("n,threshold_a", [(64 * 1024, 20316), (64 * 4096, 16384), (64, 20316),
+                                           (12_507_136, 16384)])
 def test_threshold(dm, oracle, n, threshold_a):
     rng = np.random.default_rng(DB_RNG_SEED)
     code = sample_code_dots(rng, n)
