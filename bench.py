@@ -39,10 +39,13 @@ CPU path (per-party rotation-aware dots, summed, thresholded, OR over
 rotations) on the host cores.
 
 Multi-GPU (torchrun): each rank hosts its own 524,288-entry shard of all three
-parties (global entry g on rank g % N) and processes the same query batch; the
-scan needs no collective (weak scaling); the end-to-end step merges the ranks'
-match results with one all_gather (irisb200.shard); the max step time over
-ranks is reported.
+parties (global entry g on rank g % N) and processes a query batch of the
+same shape (the same fresh queries; the planted 10% are near-duplicates of
+entries of the rank's own shard); the scan needs no collective (weak
+scaling); the end-to-end step merges the ranks' match results with one
+all_gather (irisb200.shard); the max step time over ranks is reported.  The
+secondary legs (fused scan, latency, batched, serving, sweep, CPU baselines)
+run in 1-GPU runs only.
 """
 from __future__ import annotations
 
@@ -543,7 +546,7 @@ def run_ours(args):
 
     # ---------------- fused-scan leg: the same batch, GEMM + threshold in one kernel per chunk ----------------
     fused = None
-    if not args.no_fused and n_rows % 128 == 0:
+    if world == 1 and not args.no_fused and n_rows % 128 == 0:
         dcf = irisb200.DistanceComparator(dm, NQ, M, match_list_cap=1 << 16)
 
         def fused_step():
@@ -581,7 +584,7 @@ def run_ours(args):
 
     # ---------------- latency leg: batches back to back, each bracketed by CUDA events ----------------
     latency = None
-    if args.latency_batches > 0:
+    if world == 1 and args.latency_batches > 0:
         for _ in range(args.latency_warmup):
             device_step()
         dm.synchronize()
