@@ -183,7 +183,10 @@ def test_plain_scan_every_candidate(dm, oracle, data):
         ps = PlainScan(dm, ce, me, c, dc, N_Q, N_DB, 16384)
         cands = ps.candidates()
         assert {p for p, _, _ in cands} == {"split", "pair", "fused"}
-        for cand in cands:
+        # every candidate (one chunk at this DB size), then several chunks
+        # with a ragged last one on each path (2000 = 3 x 640 + 80, 3 x 512 + 464)
+        extra = [("split", 256, 640), ("pair", 256, 512), ("fused", 128, 640), ("split", 128, 512)]
+        for cand in cands + extra:
             ps.configure(cand)
             dc.reset()
             ps.scan()
