@@ -153,7 +153,8 @@ def test_pipelined_batches_match_one_at_a_time(dm, oracle, setup):
 def test_batched_every_tuner_candidate(dm, oracle, setup, path):
     """Every (path, tile, chunk) candidate the autotuner may pick gives the CPU
     path's matches: the GEMM launch + threshold launch at each tile width, the
-    two-SM GEMM, and the one-kernel fused scan."""
+    two-SM GEMM, and the one-kernel fused scan; and each path's captured pass
+    over several chunks with a ragged last one (1024 = 2 x 384 + 256)."""
     s = setup
     c = irisb200.Circuits(dm, W.SEEDS)
     eng = BatchedEngine(dm, s["ce"], s["me"], c, max_variants=64, max_reauth=16, threshold_a=A, autotune=False,
@@ -169,6 +170,7 @@ def test_batched_every_tuner_candidate(dm, oracle, setup, path):
         assert first[0] == path
         cands = [cd for cd in BatchedEngine._candidates(n_pad, N_DB) if cd[0] == path]
         assert cands
+        cands += sorted({(p, t, 384) for p, t, _ in cands})
         for cand in cands:
             eng.tuned = {n_pad: cand}
             res = eng.run(reqs)
