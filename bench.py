@@ -901,6 +901,13 @@ def threshold_roofline(thr_ms: float, words: int, n_sm: int, sm_mhz, chunks) -> 
         ipw = pj.get("inst_per_word")
         out["inst_per_word"] = ipw
         out["counters_source"] = pj.get("source")
+        if pj.get("alu_pipe_pct") is not None:
+            # the binding pipe: integer ALU instructions issue at half the
+            # warp-instruction rate, and the kernel keeps that pipe busy
+            out["binding_pipe"] = {"pipe": "alu", "frac": pj["alu_pipe_pct"] / 100.0,
+                                   "issue_frac": pj.get("issue_active_pct", 0.0) / 100.0,
+                                   "source": "ncu sm__inst_executed_pipe_alu (pct of peak sustained active), "
+                                             "small case of the same kernel, profiles/threshold_bitmap_16k_full.md"}
         if ipw:
             out["achieved"] = ipw * words / (thr_ms * 1e-3)
     if sm_mhz:

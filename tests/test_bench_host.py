@@ -85,6 +85,11 @@ def test_percentiles_and_threshold_roofline(tmp_path, monkeypatch):
     rf = bench.threshold_roofline(10.0, 1000, 148, 1500.0, [(0, 1)])
     assert abs(rf["achieved"] - 20000.0 * 1000 / 0.01) < 1e-3
     assert abs(rf["frac"] - rf["achieved"] / rf["peak"]) < 1e-12
+    assert "binding_pipe" not in rf
+    (tmp_path / "profiles" / "threshold_bitmap_counters.json").write_text(
+        json.dumps({"inst_per_word": 20000.0, "source": "test", "alu_pipe_pct": 87.5, "issue_active_pct": 71.0}))
+    rf = bench.threshold_roofline(10.0, 1000, 148, 1500.0, [(0, 1)])
+    assert rf["binding_pipe"]["pipe"] == "alu" and abs(rf["binding_pipe"]["frac"] - 0.875) < 1e-12
 
 
 def test_cpu_mpc_simulation_matches_plaintext():
