@@ -772,17 +772,28 @@ def run_ours(args):
         ops_launch = ops * chunks[0][1] / M  # per GEMM launch (one chunk)
         gemm_avg = statistics.mean(gemm_ms)  # per batch = sum over its chunk launches
         achieved = ops / (gemm_avg * 1e-3) / 1e12  # = ops per launch / mean launch duration
-        traffic = None
+        traffic = traffic_source = None
+        # algorithmic DRAM bytes of one launch: the six engines' DB limb planes
+        # once, their query planes once, the u16 dot shares written
+        alg_bytes = (chunks[0][1] * 3 * 2 * (K_CODE + K_MASK) + 3 * n_rows * (K_CODE + K_MASK) * 2
+                     + chunks[0][1] * n_rows * 2 * 6)
         prof = os.path.join(ROOT, "profiles", "gemm_limb_traffic.json")
         if os.path.exists(prof):
             with open(prof) as f:
                 pj = json.load(f)
-            # the profile's launch covers `entries` DB entries; DRAM bytes grow in
-            # proportion to the entries a launch scans (one query-plane re-read per
-            # sweep of the SMs over the DB slabs), so scale to this launch
-            lg = pj.get({"split": "limb_gemm", "pair": "limb_gemm_pair", "fused": "fused_scan"}[chosen[0]], {})
-            if lg.get("dram_bytes_per_launch") and lg.get("entries"):
+            # a capture of this launch's own chunk length when the profile has
+            # one; else the path's capture scaled by the entries a launch scans
+            # (an estimate: the query planes' share of the bytes changes with it)
+            key = {"split": "limb_gemm", "pair": "limb_gemm_pair", "fused": "fused_scan"}[chosen[0]]
+            own = pj.get(key + "_by_chunk", {}).get(str(chunks[0][1]), {})
+            lg = pj.get(key, {})
+            if own.get("dram_bytes_per_launch"):
+                traffic = own["dram_bytes_per_launch"]
+                traffic_source = f"ncu capture of a {chunks[0][1]}-entry launch (profiles/gemm_limb_traffic.json)"
+            elif lg.get("dram_bytes_per_launch") and lg.get("entries"):
                 traffic = lg["dram_bytes_per_launch"] * chunks[0][1] / lg["entries"]
+                traffic_source = (f"ncu capture of a {lg['entries']}-entry launch scaled to {chunks[0][1]} entries "
+                                  "(profiles/gemm_limb_traffic.json)")
         thr_avg = statistics.mean(thr_ms)
         mhz = clk_value.get("sm_mhz")
         n_sm = dm.sm_count()
@@ -816,7 +827,8 @@ def run_ours(args):
             "cycles_per_batch": cycles,
             "rows_x_entries_per_s": NQ * 31 * M * world / (per_step * 1e-3),
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": None, "unit": "TOPS",
-                         "frac": None, "traffic": traffic,
+                         "frac": None, "traffic": traffic, "traffic_source": traffic_source,
+                         "algorithmic_bytes_per_launch": alg_bytes,
                          "kernel": {"split": "limb_gemm_kernel<256>", "pair": "limb_gemm_pair_kernel (cta_group::2)",
                                     "fused": "fused_scan_kernel (GEMM and threshold: time includes the threshold)"}
                                    [chosen[0]] + f" (6 engines, one launch per {chunks[0][1]}-entry DB chunk, "
