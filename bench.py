@@ -488,15 +488,12 @@ def run_ours(args):
     ps = PlainScan(dm, ce, me, c, dc, NQ, M, A)
     chunk = args.db_chunk if 0 < args.db_chunk < M else M
 
-    def scan(ev=None):
-        if ev:
-            ps.scan(events=[[(lambda e=e: e.record(s0)) for e in trio] for trio in ev])
-        else:
-            ps.scan()
+    def scan():
+        ps.scan()
 
-    def device_step(ev=None):
+    def device_step():
         dc.reset()
-        scan(ev)
+        scan()
 
     clk = ClockSampler(local).__enter__()
     time.sleep(2.0)  # let nvidia-smi initialise before anything is timed
@@ -514,7 +511,9 @@ def run_ours(args):
     dm.synchronize()
 
     # ---------------- device-resident timing ----------------
-    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in chunks] for _ in range(args.steps)]
+    # per-chunk CUDA events of the library's DB pass, on the launching stream:
+    # before each chunk, after its GEMM (or fused launch), after its threshold
+    ps.set_timing(args.steps)
     begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
         dist.barrier()
@@ -523,15 +522,14 @@ def run_ours(args):
     with clk.mark():
         begin.record(s0)
         for i in range(args.steps):
-            device_step(evs[i])
+            device_step()
         end.record(s0)
         end.synchronize()
     dm.synchronize()
     clk_value = clk.summary(clk.windows[-1])
     total_ms = begin.elapsed_time(end)
-    gemm_ms = [sum(e[0].elapsed_time(e[1]) for e in evs[i]) for i in range(args.steps)]  # per step, all chunks
-    thr_ms = [sum(e[1].elapsed_time(e[2]) for e in evs[i]) for i in range(args.steps)]
-    batch_ms = [evs[i][0][0].elapsed_time(evs[i][-1][2]) for i in range(args.steps)]
+    gemm_ms, thr_ms, batch_ms = ps.timings()  # per step, summed over its chunks
+    ps.set_timing(0)
     if dist:
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -643,6 +641,7 @@ def run_ours(args):
     e2e_value = comps * args.steps / e2e_s
 
     ps.restore()
+    ps.close()
     # ---------------- batched uneven leg (same engines, same DB) ----------------
     batched = None
     if reqs:

@@ -480,6 +480,71 @@ int irs_dc_fetch_final_results(irs_distance_comparator* dc, size_t n_queries, ui
                                uint32_t* match_counters, uint32_t* all_matches);
 
 /* ------------------------------------------------------------------------ */
+/* The plain DB pass and its autotuner: the chunk loop of                    */
+/* compare_query_against_db_and_self_prefiltering (actor.rs:2246-2589) over  */
+/* the resident engines for one uploaded batch of n_slots 32-row query slots */
+/* (rows 0..30 valid, slot s reported as query s) and entries [0, db_len).   */
+/* Per chunk one of three paths: the limb GEMM launch then the threshold     */
+/* launch (IRS_SCAN_SPLIT, at a tile width), the same with the two-SM GEMM   */
+/* (IRS_SCAN_PAIR, 256-row tile), or irs_dc_scan_fused (IRS_SCAN_FUSED).     */
+/* Results are identical on every path; irs_scan_tune times each candidate   */
+/* on the batch (the choice cuBLAS makes inside the reference's dots).      */
+/* ------------------------------------------------------------------------ */
+typedef struct irs_scan irs_scan;
+enum { IRS_SCAN_SPLIT = 0, IRS_SCAN_PAIR = 1, IRS_SCAN_FUSED = 2 };
+typedef struct irs_scan_candidate {
+  int32_t path;   /* IRS_SCAN_SPLIT, IRS_SCAN_PAIR or IRS_SCAN_FUSED */
+  int32_t tile;   /* GEMM query-row tile width (256, 128, 64; 128 for the fused kernel) */
+  uint64_t chunk; /* DB entries per chunk (a multiple of 32) */
+} irs_scan_candidate;
+typedef struct irs_scan_timing {
+  irs_scan_candidate cand;
+  double ms;        /* host wall time per pass, device synchronised */
+  int32_t finalist; /* 0: the first round; 1: a finalist's mean over the interleaved rounds */
+  int32_t reserved;
+} irs_scan_timing;
+/* The engines are the three parties' code and mask engines (party p at index
+ * p); the scan keeps the handles, which must outlive it.  Starts configured
+ * as IRS_SCAN_SPLIT with the engines' own tile, 65,536-entry chunks. */
+int irs_scan_init(irs_device_manager* dm, irs_distance_comparator* dc, irs_circuits* c,
+                  irs_sharedb* const code_engines[3], irs_sharedb* const mask_engines[3], size_t n_slots,
+                  size_t db_len, uint32_t threshold_a, irs_scan** out);
+int irs_scan_destroy(irs_scan* s);
+/* The tuner's candidates for this batch shape: the two-launch path at every
+ * tile width that divides the padded rows (64 only up to 768 rows), the
+ * two-SM GEMM where the 256-row tile applies, the fused kernel where the rows
+ * are a multiple of 128; chunks of 131,072 down to 8,192 entries capped at
+ * the DB (the fused kernel on the three longest).  *n = the count; at most
+ * cap are written. */
+int irs_scan_candidates(irs_scan* s, irs_scan_candidate* out, size_t cap, size_t* n);
+/* Sets every engine's GEMM variant and tile for the path (set_pair /
+ * set_tile) and the chunk length; the fused path allocates the comparator's
+ * ring here, so configure it before any graph capture.  Clears the timing
+ * events. */
+int irs_scan_configure(irs_scan* s, int path, int tile, size_t chunk);
+int irs_scan_current(irs_scan* s, irs_scan_candidate* cand);
+/* One pass over the DB (the comparator is not reset) on `stream` (NULL =
+ * party 0's stream). */
+int irs_scan_run(irs_scan* s, void* stream);
+/* Per-chunk timing of the next max_passes passes (0 = off): CUDA events
+ * before each chunk, after its GEMM (or fused launch) and after its
+ * threshold launch, on the pass's stream.  irs_scan_timings waits for them
+ * and writes per pass the GEMM, threshold and whole-pass milliseconds (*n =
+ * passes recorded; reset != 0 starts over). */
+int irs_scan_set_timing(irs_scan* s, size_t max_passes);
+int irs_scan_timings(irs_scan* s, double* gemm_ms, double* threshold_ms, double* pass_ms, size_t cap, size_t* n,
+                     int reset);
+/* Times `passes` consecutive passes of every candidate after a warm one
+ * (comparator reset before each), re-times the `finalists` fastest
+ * interleaved for `rounds` rounds and configures the best mean; `log`
+ * receives the first-round times, then each finalist's mean (*n_log = the
+ * count; at most log_cap written). */
+int irs_scan_tune(irs_scan* s, int passes, int finalists, int rounds, irs_scan_candidate* chosen,
+                  irs_scan_timing* log, size_t log_cap, size_t* n_log);
+/* The engines back to the library's default GEMM (set_pair 0, set_tile 0). */
+int irs_scan_restore(irs_scan* s);
+
+/* ------------------------------------------------------------------------ */
 /* CUDA graphs of a batch's device work (party 0's stream).  No counterpart */
 /* in the reference, which launches every kernel through cudarc.            */
 /* Between begin and end, the library keeps all launches on the capturing    */

@@ -13,8 +13,16 @@ use std::ffi::{c_char, c_int, c_void, CStr};
 #[repr(C)] pub struct IrsCircuits { _p: [u8; 0] }
 #[repr(C)] pub struct IrsDistanceComparator { _p: [u8; 0] }
 #[repr(C)] pub struct IrsGraph { _p: [u8; 0] }
+#[repr(C)] pub struct IrsScan { _p: [u8; 0] }
 #[repr(C)] #[derive(Clone, Copy)]
 pub struct IrsQuerySlot { pub src: u32, pub rot_lo: u32, pub n_rot: u32, pub query: u32 }
+pub const IRS_SCAN_SPLIT: i32 = 0;
+pub const IRS_SCAN_PAIR: i32 = 1;
+pub const IRS_SCAN_FUSED: i32 = 2;
+#[repr(C)] #[derive(Clone, Copy)]
+pub struct IrsScanCandidate { pub path: i32, pub tile: i32, pub chunk: u64 }
+#[repr(C)] #[derive(Clone, Copy)]
+pub struct IrsScanTiming { pub cand: IrsScanCandidate, pub ms: f64, pub finalist: i32, pub reserved: i32 }
 
 #[link(name = "irisb200")]
 extern "C" {
@@ -131,6 +139,20 @@ extern "C" {
     pub fn irs_dc_scan_fused(dc: *mut IrsDistanceComparator, c: *mut IrsCircuits,
         code_engines: *const *mut IrsShareDb, mask_engines: *const *mut IrsShareDb, offset: usize,
         len: usize, n_slots: usize, threshold_a: u32, use_segments: c_int, stream: *mut c_void) -> c_int;
+    pub fn irs_scan_init(dm: *mut IrsDeviceManager, dc: *mut IrsDistanceComparator, c: *mut IrsCircuits,
+        code_engines: *const *mut IrsShareDb, mask_engines: *const *mut IrsShareDb, n_slots: usize,
+        db_len: usize, threshold_a: u32, out: *mut *mut IrsScan) -> c_int;
+    pub fn irs_scan_destroy(s: *mut IrsScan) -> c_int;
+    pub fn irs_scan_candidates(s: *mut IrsScan, out: *mut IrsScanCandidate, cap: usize, n: *mut usize) -> c_int;
+    pub fn irs_scan_configure(s: *mut IrsScan, path: c_int, tile: c_int, chunk: usize) -> c_int;
+    pub fn irs_scan_current(s: *mut IrsScan, cand: *mut IrsScanCandidate) -> c_int;
+    pub fn irs_scan_run(s: *mut IrsScan, stream: *mut c_void) -> c_int;
+    pub fn irs_scan_set_timing(s: *mut IrsScan, max_passes: usize) -> c_int;
+    pub fn irs_scan_timings(s: *mut IrsScan, gemm_ms: *mut f64, threshold_ms: *mut f64, pass_ms: *mut f64,
+        cap: usize, n: *mut usize, reset: c_int) -> c_int;
+    pub fn irs_scan_tune(s: *mut IrsScan, passes: c_int, finalists: c_int, rounds: c_int,
+        chosen: *mut IrsScanCandidate, log: *mut IrsScanTiming, log_cap: usize, n_log: *mut usize) -> c_int;
+    pub fn irs_scan_restore(s: *mut IrsScan) -> c_int;
     pub fn irs_dc_take_rows(dc: *mut IrsDistanceComparator, rows: *const u32, n: usize,
         db_len: usize, clear: c_int, counts: *mut u32, ids: *mut u32) -> c_int;
     pub fn irs_dc_enable_distance_capture(dc: *mut IrsDistanceComparator, cap: usize) -> c_int;

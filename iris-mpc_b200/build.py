@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "irisb200")
 LIB = os.path.join(OUT_DIR, "libirisb200.so")
 SOURCES = ["capi.cu", "gemm_limb.cu", "threshold.cu", "prep.cu", "results.cu", "host_galois.cu", "noalloc.cu",
-           "or_tree.cu", "fused_scan.cu"]
+           "or_tree.cu", "fused_scan.cu", "scan.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O3",
          "-Xptxas", "-warn-spills"]

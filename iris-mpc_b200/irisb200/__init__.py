@@ -47,6 +47,17 @@ class QuerySlot(C.Structure):
     _fields_ = [("src", C.c_uint32), ("rot_lo", C.c_uint32), ("n_rot", C.c_uint32), ("query", C.c_uint32)]
 
 
+SCAN_PATHS = ("split", "pair", "fused")  # IRS_SCAN_SPLIT, IRS_SCAN_PAIR, IRS_SCAN_FUSED
+
+
+class ScanCandidate(C.Structure):
+    _fields_ = [("path", C.c_int32), ("tile", C.c_int32), ("chunk", C.c_uint64)]
+
+
+class ScanTiming(C.Structure):
+    _fields_ = [("cand", ScanCandidate), ("ms", C.c_double), ("finalist", C.c_int32), ("reserved", C.c_int32)]
+
+
 _vp = C.c_void_p
 _sz = C.c_size_t
 _u32 = C.c_uint32
@@ -119,6 +130,16 @@ _SIGS = {
     "irs_dc_set_segments": [_vp, _sz, _vp, _vp, _vp],
     "irs_dc_compare_threshold_open_prepared": [_vp, _vp, _vp, _vp, _sz, _sz, _u32, _i, _vp],
     "irs_dc_scan_fused": [_vp, _vp, _vp, _vp, _sz, _sz, _sz, _u32, _i, _vp],
+    "irs_scan_init": [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _u32, C.POINTER(_vp)],
+    "irs_scan_destroy": [_vp],
+    "irs_scan_candidates": [_vp, C.POINTER(ScanCandidate), _sz, C.POINTER(_sz)],
+    "irs_scan_configure": [_vp, _i, _i, _sz],
+    "irs_scan_current": [_vp, C.POINTER(ScanCandidate)],
+    "irs_scan_run": [_vp, _vp],
+    "irs_scan_set_timing": [_vp, _sz],
+    "irs_scan_timings": [_vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), _i],
+    "irs_scan_tune": [_vp, _i, _i, _i, C.POINTER(ScanCandidate), C.POINTER(ScanTiming), _sz, C.POINTER(_sz)],
+    "irs_scan_restore": [_vp],
     "irs_graph_begin_capture": [_vp],
     "irs_graph_end_capture": [_vp, C.POINTER(_vp)],
     "irs_graph_launch": [_vp, _vp],

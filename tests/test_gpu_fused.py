@@ -193,8 +193,36 @@ def test_plain_scan_every_candidate(dm, oracle, data):
             dm.synchronize()
             got = irisb200.bitmap_get(dc.fetch_bitmap(N_Q, N_DB), N_Q, N_DB)
             assert np.array_equal(got, exp), f"candidate {cand}"
+        # per-chunk timing of the configured path: one entry per timed pass
+        for cand in (("pair", 256, 512), ("fused", 128, 640)):
+            ps.configure(cand)
+            ps.set_timing(2)
+            for _ in range(3):  # the third pass is past the timing capacity
+                dc.reset()
+                ps.scan()
+            g, t, whole = ps.timings()
+            assert len(g) == len(t) == len(whole) == 2
+            for x, y, z in zip(g, t, whole):
+                assert x > 0 and z >= x + y - 1e-3
+                # the fused launch is the chunk's whole work: nothing between its two later events
+                assert y < 0.1 if cand[0] == "fused" else y > 0
+            got = irisb200.bitmap_get(dc.fetch_bitmap(N_Q, N_DB), N_Q, N_DB)
+            assert np.array_equal(got, exp), f"timed {cand}"
+        # the tuner: every candidate once, the three fastest re-timed, the best
+        # finalist mean configured; results unchanged afterwards
         best = ps.tune()
-        assert best in cands and len(ps.tune_log) == len(cands) + min(3, len(cands))
+        n = len(cands)
+        assert best in cands and len(ps.tune_log) == n + min(3, n) and ps.cand == best
+        first = sorted(ps.tune_log[:n], key=lambda x: x[1])
+        finals = ps.tune_log[n:]
+        assert [cd for cd, _ in finals] == [cd for cd, _ in first[:3]]
+        assert best == min(finals, key=lambda x: x[1])[0]
+        dc.reset()
+        ps.scan()
+        dm.synchronize()
+        got = irisb200.bitmap_get(dc.fetch_bitmap(N_Q, N_DB), N_Q, N_DB)
+        assert np.array_equal(got, exp), f"tuned {best}"
         ps.restore()
+        ps.close()
     finally:
         _close([dc, c] + ce + me)
