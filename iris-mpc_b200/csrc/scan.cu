@@ -167,10 +167,11 @@ int irs_scan_run(irs_scan* s, void* stream) {
   }
   cudaStream_t cs = static_cast<cudaStream_t>(st);
   const size_t nc = n_chunks(s);
+  // a timed pass counts once all its launches are enqueued; a failed one
+  // leaves its slot to the next pass
   cudaEvent_t* ev = nullptr;
   if (s->per_pass && s->passes < s->max_passes) {
     ev = &s->ev[s->passes * s->per_pass];
-    s->passes++;
     if (cudaEventRecord(ev[0], cs) != cudaSuccess) {
       cudaGetLastError();
       return set_error(IRS_ERR_CUDA, "timing event record failed");
@@ -193,6 +194,7 @@ int irs_scan_run(irs_scan* s, void* stream) {
     if (rc) return rc;
     if (ev) cudaEventRecord(ev[2 + 2 * k], cs);
   }
+  if (ev) s->passes++;
   return IRS_OK;
 }
 
@@ -226,14 +228,19 @@ int irs_scan_timings(irs_scan* s, double* gemm_ms, double* threshold_ms, double*
       return set_error(IRS_ERR_CUDA, "timing event wait failed");
     }
     double g = 0.0, t = 0.0;
-    float x = 0.0f;
+    float x = 0.0f, y = 0.0f;
+    bool ok = true;
     for (size_t k = 0; k < nc; k++) {
-      cudaEventElapsedTime(&x, ev[2 * k], ev[1 + 2 * k]);  // GEMM (or the fused launch)
+      ok = ok && cudaEventElapsedTime(&x, ev[2 * k], ev[1 + 2 * k]) == cudaSuccess;  // GEMM (or the fused launch)
+      ok = ok && cudaEventElapsedTime(&y, ev[1 + 2 * k], ev[2 + 2 * k]) == cudaSuccess;  // threshold, open, OR
       g += x;
-      cudaEventElapsedTime(&x, ev[1 + 2 * k], ev[2 + 2 * k]);  // threshold, open, OR
-      t += x;
+      t += y;
     }
-    cudaEventElapsedTime(&x, ev[0], ev[2 * nc]);
+    ok = ok && cudaEventElapsedTime(&x, ev[0], ev[2 * nc]) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      return set_error(IRS_ERR_CUDA, "reading the timing events of pass %zu failed", p);
+    }
     gemm_ms[p] = g;
     threshold_ms[p] = t;
     pass_ms[p] = x;
