@@ -517,6 +517,12 @@ int irs_scan_destroy(irs_scan* s);
  * the DB (the fused kernel on the three longest).  *n = the count; at most
  * cap are written. */
 int irs_scan_candidates(irs_scan* s, irs_scan_candidate* out, size_t cap, size_t* n);
+/* Packed uneven rows instead of plain slots: the candidates are for n_rows
+ * padded query rows (0 = n_slots x 32) and, with use_segments != 0, every
+ * pass evaluates the threshold through the comparator's stored segment table
+ * (irs_dc_set_segments; irs_dc_compare_threshold_open_prepared, or the fused
+ * kernel with use_segments), as BatchedEngine packs its variants. */
+int irs_scan_set_rows(irs_scan* s, size_t n_rows, int use_segments);
 /* Sets every engine's GEMM variant and tile for the path (set_pair /
  * set_tile) and the chunk length; the fused path allocates the comparator's
  * ring here, so configure it before any graph capture.  Clears the timing
@@ -524,7 +530,9 @@ int irs_scan_candidates(irs_scan* s, irs_scan_candidate* out, size_t cap, size_t
 int irs_scan_configure(irs_scan* s, int path, int tile, size_t chunk);
 int irs_scan_current(irs_scan* s, irs_scan_candidate* cand);
 /* One pass over the DB (the comparator is not reset) on `stream` (NULL =
- * party 0's stream). */
+ * party 0's stream); graph-capturable on party 0's stream when timing is
+ * off and the configuration (and, for the fused path, its ring) was made
+ * before the capture. */
 int irs_scan_run(irs_scan* s, void* stream);
 /* Per-chunk timing of the next max_passes passes (0 = off): CUDA events
  * before each chunk, after its GEMM (or fused launch) and after its
@@ -534,12 +542,12 @@ int irs_scan_run(irs_scan* s, void* stream);
 int irs_scan_set_timing(irs_scan* s, size_t max_passes);
 int irs_scan_timings(irs_scan* s, double* gemm_ms, double* threshold_ms, double* pass_ms, size_t cap, size_t* n,
                      int reset);
-/* Times `passes` consecutive passes of every candidate after a warm one
- * (comparator reset before each), re-times the `finalists` fastest
- * interleaved for `rounds` rounds and configures the best mean; `log`
- * receives the first-round times, then each finalist's mean (*n_log = the
- * count; at most log_cap written). */
-int irs_scan_tune(irs_scan* s, int passes, int finalists, int rounds, irs_scan_candidate* chosen,
+/* Times `passes` consecutive passes of every candidate (only those on path
+ * `only_path` when >= 0) after a warm one (comparator reset before each),
+ * re-times the `finalists` fastest interleaved for `rounds` rounds and
+ * configures the best mean; `log` receives the first-round times, then each
+ * finalist's mean (*n_log = the count; at most log_cap written). */
+int irs_scan_tune(irs_scan* s, int passes, int finalists, int rounds, int only_path, irs_scan_candidate* chosen,
                   irs_scan_timing* log, size_t log_cap, size_t* n_log);
 /* The engines back to the library's default GEMM (set_pair 0, set_tile 0). */
 int irs_scan_restore(irs_scan* s);

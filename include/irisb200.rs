@@ -144,13 +144,14 @@ extern "C" {
         db_len: usize, threshold_a: u32, out: *mut *mut IrsScan) -> c_int;
     pub fn irs_scan_destroy(s: *mut IrsScan) -> c_int;
     pub fn irs_scan_candidates(s: *mut IrsScan, out: *mut IrsScanCandidate, cap: usize, n: *mut usize) -> c_int;
+    pub fn irs_scan_set_rows(s: *mut IrsScan, n_rows: usize, use_segments: c_int) -> c_int;
     pub fn irs_scan_configure(s: *mut IrsScan, path: c_int, tile: c_int, chunk: usize) -> c_int;
     pub fn irs_scan_current(s: *mut IrsScan, cand: *mut IrsScanCandidate) -> c_int;
     pub fn irs_scan_run(s: *mut IrsScan, stream: *mut c_void) -> c_int;
     pub fn irs_scan_set_timing(s: *mut IrsScan, max_passes: usize) -> c_int;
     pub fn irs_scan_timings(s: *mut IrsScan, gemm_ms: *mut f64, threshold_ms: *mut f64, pass_ms: *mut f64,
         cap: usize, n: *mut usize, reset: c_int) -> c_int;
-    pub fn irs_scan_tune(s: *mut IrsScan, passes: c_int, finalists: c_int, rounds: c_int,
+    pub fn irs_scan_tune(s: *mut IrsScan, passes: c_int, finalists: c_int, rounds: c_int, only_path: c_int,
         chosen: *mut IrsScanCandidate, log: *mut IrsScanTiming, log_cap: usize, n_log: *mut usize) -> c_int;
     pub fn irs_scan_restore(s: *mut IrsScan) -> c_int;
     pub fn irs_dc_take_rows(dc: *mut IrsDistanceComparator, rows: *const u32, n: usize,

@@ -26,6 +26,8 @@ struct irs_scan {
   irs_sharedb* me[3] = {nullptr, nullptr, nullptr};
   irs_sharedb* all[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   size_t n_slots = 0, db_len = 0;
+  size_t n_rows = 0;      // padded query rows the candidates are for (0: n_slots x 32)
+  bool segments = false;  // threshold via the comparator's stored segment table
   uint32_t threshold_a = 0;
   irs_scan_candidate cand{IRS_SCAN_SPLIT, 0, 65536};
   // per-chunk timing events (irs_scan_set_timing): per pass, the start and
@@ -108,7 +110,7 @@ int irs_scan_destroy(irs_scan* s) {
 
 int irs_scan_candidates(irs_scan* s, irs_scan_candidate* out, size_t cap, size_t* n) {
   if (!s || !n || (cap && !out)) return set_error(IRS_ERR_INVALID, "bad arguments");
-  const uint64_t rows = (uint64_t)s->n_slots * IRS_SLOT_ROWS;
+  const uint64_t rows = s->n_rows ? (uint64_t)s->n_rows : (uint64_t)s->n_slots * IRS_SLOT_ROWS;
   const uint64_t n_pad = (rows + 63) / 64 * 64;
   const uint64_t full = (s->db_len + 31) / 32 * 32;
   std::vector<uint64_t> chunks;
@@ -144,11 +146,18 @@ int irs_scan_configure(irs_scan* s, int path, int tile, size_t chunk) {
     if (rc) return rc;
   }
   if (path == IRS_SCAN_FUSED) {  // allocates the comparator's ring before any capture
-    int rc = irs_dc_scan_fused(s->dc, s->c, s->ce, s->me, 0, 0, s->n_slots, s->threshold_a, 0, nullptr);
+    int rc = irs_dc_scan_fused(s->dc, s->c, s->ce, s->me, 0, 0, s->n_slots, s->threshold_a, s->segments, nullptr);
     if (rc) return rc;
   }
   s->cand = {path, tile, (uint64_t)chunk};
   free_events(s);  // the timing events are laid out for a chunk count
+  return IRS_OK;
+}
+
+int irs_scan_set_rows(irs_scan* s, size_t n_rows, int use_segments) {
+  if (!s) return set_error(IRS_ERR_INVALID, "scan is NULL");
+  s->n_rows = n_rows;
+  s->segments = use_segments != 0;
   return IRS_OK;
 }
 
@@ -182,14 +191,16 @@ int irs_scan_run(irs_scan* s, void* stream) {
     const size_t len = std::min<size_t>(s->cand.chunk, s->db_len - off);
     int rc;
     if (s->cand.path == IRS_SCAN_FUSED) {
-      rc = irs_dc_scan_fused(s->dc, s->c, s->ce, s->me, off, len, s->n_slots, s->threshold_a, 0, st);
+      rc = irs_dc_scan_fused(s->dc, s->c, s->ce, s->me, off, len, s->n_slots, s->threshold_a, s->segments, st);
       if (!rc && ev) cudaEventRecord(ev[1 + 2 * k], cs);
     } else {
       rc = irs_sharedb_dot_many(s->all, kMults, 6, off, len, st);
       if (!rc && ev) cudaEventRecord(ev[1 + 2 * k], cs);
       if (!rc)
-        rc = irs_dc_compare_threshold_open(s->dc, s->c, s->ce, s->me, off, len, s->n_slots, nullptr, nullptr,
-                                           s->threshold_a, 0, st);
+        rc = s->segments ? irs_dc_compare_threshold_open_prepared(s->dc, s->c, s->ce, s->me, off, len,
+                                                                  s->threshold_a, 0, st)
+                         : irs_dc_compare_threshold_open(s->dc, s->c, s->ce, s->me, off, len, s->n_slots, nullptr,
+                                                         nullptr, s->threshold_a, 0, st);
     }
     if (rc) return rc;
     if (ev) cudaEventRecord(ev[2 + 2 * k], cs);
@@ -249,7 +260,7 @@ int irs_scan_timings(irs_scan* s, double* gemm_ms, double* threshold_ms, double*
   return IRS_OK;
 }
 
-int irs_scan_tune(irs_scan* s, int passes, int finalists, int rounds, irs_scan_candidate* chosen,
+int irs_scan_tune(irs_scan* s, int passes, int finalists, int rounds, int only_path, irs_scan_candidate* chosen,
                   irs_scan_timing* log, size_t log_cap, size_t* n_log) {
   if (!s || !chosen || (log_cap && !log)) return set_error(IRS_ERR_INVALID, "bad arguments");
   if (passes < 1 || finalists < 1 || rounds < 0) return set_error(IRS_ERR_INVALID, "passes, finalists >= 1, rounds >= 0");
@@ -258,6 +269,14 @@ int irs_scan_tune(irs_scan* s, int passes, int finalists, int rounds, irs_scan_c
   if (rc) return rc;
   std::vector<irs_scan_candidate> cands(nc);
   if ((rc = irs_scan_candidates(s, cands.data(), nc, &nc))) return rc;
+  if (only_path >= 0) {
+    std::vector<irs_scan_candidate> keep;
+    for (const irs_scan_candidate& c : cands)
+      if (c.path == only_path) keep.push_back(c);
+    if (keep.empty()) return set_error(IRS_ERR_INVALID, "no candidate on path %d for this batch shape", only_path);
+    cands.swap(keep);
+    nc = cands.size();
+  }
   size_t nl = 0;
   auto note = [&](const irs_scan_candidate& c, double ms, int finalist) {
     if (nl < log_cap) log[nl] = {c, ms, finalist, 0};

@@ -133,12 +133,13 @@ _SIGS = {
     "irs_scan_init": [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _u32, C.POINTER(_vp)],
     "irs_scan_destroy": [_vp],
     "irs_scan_candidates": [_vp, C.POINTER(ScanCandidate), _sz, C.POINTER(_sz)],
+    "irs_scan_set_rows": [_vp, _sz, _i],
     "irs_scan_configure": [_vp, _i, _i, _sz],
     "irs_scan_current": [_vp, C.POINTER(ScanCandidate)],
     "irs_scan_run": [_vp, _vp],
     "irs_scan_set_timing": [_vp, _sz],
     "irs_scan_timings": [_vp, _vp, _vp, _vp, _sz, C.POINTER(_sz), _i],
-    "irs_scan_tune": [_vp, _i, _i, _i, C.POINTER(ScanCandidate), C.POINTER(ScanTiming), _sz, C.POINTER(_sz)],
+    "irs_scan_tune": [_vp, _i, _i, _i, _i, C.POINTER(ScanCandidate), C.POINTER(ScanTiming), _sz, C.POINTER(_sz)],
     "irs_scan_restore": [_vp],
     "irs_graph_begin_capture": [_vp],
     "irs_graph_end_capture": [_vp, C.POINTER(_vp)],

@@ -14,10 +14,12 @@ prefetch_subset share_db.rs:344-407) instead of the whole DB.
 
 The device work of a batch -- comparator reset, the six limb GEMMs and the
 fused threshold/open/OR per DB chunk, the result merge -- is captured once per
-layout into a CUDA graph and replayed; the ChaCha batch id comes from the
-device batch counter, so a replay draws fresh randomness.  The autotuner picks,
-per padded row count, by timing each candidate's captured pass (and the three
-fastest again, interleaved, against the clock's drift): the path
+layout into a CUDA graph and replayed (the DB pass itself is the library's
+native irs_scan_run over the segment table); the ChaCha batch id comes from
+the device batch counter, so a replay draws fresh randomness.  The library's
+native tuner (irs_scan_tune) picks, per padded row count, by timing each
+candidate's pass (and the three fastest again, interleaved, against the
+clock's drift): the path
 (the GEMM launch then the threshold launch per chunk, the same with the two-SM
 GEMM, or the one-kernel fused GEMM + threshold scan), the GEMM's tile width
 along the query rows and the DB chunk length.
@@ -29,13 +31,13 @@ two batches can be in flight; collect() returns a batch's results.
 """
 from __future__ import annotations
 
-import time
 from dataclasses import dataclass, field
 
 import numpy as np
 
 from . import (IRIS_CODE_LENGTH, MASK_CODE_LENGTH, MAX_MATCHES_LEN, Circuits, DeviceManager, DistanceComparator,
                Event, Graph, IrisError, PinnedArray, ShareDB, dot_many)
+from .scan import PlainScan
 
 MULTS = [1, 1, 1, 2, 2, 2]
 
@@ -200,6 +202,8 @@ class BatchedEngine:
         self._inflight = [None, None]
         self._par = 0
         self.graphs = {}
+        # the DB pass and its tuner, native (irs_scan_*), over the packed rows
+        self.scan = PlainScan(dm, self.ce, self.me, circuits, self.dc, 1, self.db_len, threshold_a)
         self.tuned = {}       # padded rows -> chosen (path, tile, chunk)
         self.tune_log = {}    # padded rows -> [(candidate, ms per DB pass)]
         self.autotune = autotune
@@ -216,17 +220,12 @@ class BatchedEngine:
             off += ln
         return out
 
-    def _capture(self, n_slots: int, path: str, chunk: int) -> Graph:
-        engines = self.ce + self.me
-
+    def _capture(self) -> Graph:
+        """The DB pass of the configured candidate as a graph: comparator
+        reset, the library's native pass (irs_scan_run, segment table), merge."""
         def body():
             self.dc.reset()
-            for off, ln in self._chunks(self.db_len, chunk):
-                if path == "fused":
-                    self.dc.scan_fused(self.c, self.ce, self.me, off, ln, self.threshold_a, use_segments=True)
-                else:
-                    dot_many(engines, MULTS, off, ln)
-                    self.dc.compare_threshold_open_prepared(self.c, self.ce, self.me, off, ln, self.threshold_a)
+            self.scan.scan()
             self.dc.join_db_matches(self.max_variants, self.db_len)
         return Graph.capture(self.dm, body)
 
@@ -255,24 +254,25 @@ class BatchedEngine:
             out += [("fused", 128, ch) for ch in chunks[:3]]
         return out
 
-    def _configure(self, path: str, tile: int) -> None:
-        for e in self.ce + self.me:
-            e.set_pair(path == "pair")
-            e.set_tile(tile if path != "fused" else 0)
-
     def _run_db_pass(self, layout: Layout, cand) -> None:
         path, tile, chunk = cand
         key = (layout.n_slots, path, tile, chunk, self.db_len)
-        self._configure(path, tile)
+        self.scan.set_rows(layout.n_rows, True)
+        self.scan.configure(cand)  # engines' GEMM variant and tile; the fused ring before any capture
         g = self.graphs.get(key)
         if g is None:
-            if path == "fused":  # allocates the comparator's ring outside the capture
-                self.dc.scan_fused(self.c, self.ce, self.me, 0, 0, self.threshold_a, use_segments=True)
-            g = self._capture(layout.n_slots, path, chunk)
+            g = self._capture()
             self.graphs[key] = g
         g.launch(self.dm.stream(0))
 
     def _tune(self, layout: Layout):
+        """The (path, tile, chunk) for this padded row count: the library's
+        native tuner (irs_scan_tune) times every candidate on the batch at hand
+        -- a warm pass, then two consecutive passes each (the power-capped
+        clock needs them to settle) -- then re-times the three fastest
+        interleaved over two rounds (the clock drifts during a tuning run by as
+        much as the candidates differ) and keeps the best mean; once per
+        padded row count."""
         n_pad = (layout.n_rows + 63) // 64 * 64
         if n_pad in self.tuned:
             return self.tuned[n_pad]
@@ -282,35 +282,10 @@ class BatchedEngine:
         if not self.autotune or len(cands) == 1:
             self.tuned[n_pad] = cands[0]
             return cands[0]
-        def timed(cand) -> float:
-            self._run_db_pass(layout, cand)  # warm (and capture)
-            self.dm.synchronize()
-            # consecutive passes: the power-capped clock settles differently for
-            # long launches and for alternating GEMM / threshold chunks, and a
-            # single pass after idle time does not show it
-            t0 = time.perf_counter()
-            for _ in range(2):
-                self._run_db_pass(layout, cand)
-            self.dm.synchronize()
-            return (time.perf_counter() - t0) / 2
-
-        self.tune_log[n_pad] = []
-        first = []
-        for cand in cands:
-            el = timed(cand)
-            first.append((el, cand))
-            self.tune_log[n_pad].append((cand, el * 1e3))
-        # the three fastest again, interleaved over two rounds: the clock drifts
-        # during a tuning run, and candidates timed far apart differ by as much
-        # as the candidates themselves
-        first.sort(key=lambda x: x[0])
-        top = [c for _, c in first[:3]]
-        acc = {c: 0.0 for c in top}
-        for _ in range(2):
-            for c in top:
-                acc[c] += timed(c)
-        self.tune_log[n_pad] += [(c, acc[c] / 2 * 1e3) for c in top]
-        best = min(top, key=lambda c: acc[c])
+        self.scan.set_rows(layout.n_rows, True)
+        only = self.fixed if any(c[0] == self.fixed for c in cands) else None
+        best = self.scan.tune(only_path=only)
+        self.tune_log[n_pad] = list(self.scan.tune_log)
         self.tuned[n_pad] = best
         return best
 
@@ -485,9 +460,8 @@ class BatchedEngine:
         for g in self.graphs.values():
             g.close()
         self.graphs.clear()
-        for e in self.ce + self.me:  # the DB engines go back to the library's default GEMM
-            e.set_pair(False)
-            e.set_tile(0)
+        self.scan.restore()  # the DB engines go back to the library's default GEMM
+        self.scan.close()
         for o in self.sce + self.sme + [self.dc, self.sdc]:
             o.close()
         for a in self._pinned:

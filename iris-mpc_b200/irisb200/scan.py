@@ -57,6 +57,11 @@ class PlainScan:
         _check(lib().irs_scan_candidates(self.h, arr, n.value, C.byref(n)))
         return [_cand(c) for c in arr]
 
+    def set_rows(self, n_rows: int, use_segments: bool) -> None:
+        """Packed uneven rows: candidates for `n_rows` padded rows (0 = the
+        slots'), and the threshold through the comparator's segment table."""
+        _check(lib().irs_scan_set_rows(self.h, n_rows, int(use_segments)))
+
     def configure(self, cand) -> None:
         path, tile, chunk = cand
         _check(lib().irs_scan_configure(self.h, SCAN_PATHS.index(path), int(tile), int(chunk)))
@@ -85,18 +90,20 @@ class PlainScan:
                                       n.value, C.byref(n), int(reset)))
         return list(g)[:n.value], list(t)[:n.value], list(p)[:n.value]
 
-    def tune(self, passes: int = 2, finalists: int = 3, rounds: int = 2):
+    def tune(self, passes: int = 2, finalists: int = 3, rounds: int = 2, only_path: str | None = None):
         """Times `passes` consecutive passes of each candidate after a warm
         pass (the power-capped clock settles differently for each path), then
         re-times the `finalists` fastest interleaved for `rounds` rounds (the
         clock drifts over a tuning run, and candidates timed far apart are not
-        comparable at the 2% level), configures the best mean and returns it.
+        comparable at the 2% level), configures the best mean and returns it;
+        `only_path` restricts the candidates to one path.
         tune_log: (candidate, ms per pass) of the first round, then
         (candidate, mean ms over the interleaved rounds) per finalist."""
         cap = len(self.candidates()) + max(0, finalists)
         log = (ScanTiming * cap)()
         chosen, n = ScanCandidate(), C.c_size_t()
-        _check(lib().irs_scan_tune(self.h, passes, finalists, rounds, C.byref(chosen), log, cap, C.byref(n)))
+        op = -1 if only_path is None else SCAN_PATHS.index(only_path)
+        _check(lib().irs_scan_tune(self.h, passes, finalists, rounds, op, C.byref(chosen), log, cap, C.byref(n)))
         self.tune_log = [(_cand(x.cand), float(x.ms)) for x in log[:min(n.value, cap)]]
         return _cand(chosen)
 

@@ -124,6 +124,7 @@ def _fake_engine(monkeypatch):
     e.sce = [_Obj(query_length=8 * 64) for _ in range(3)]
     e.sme = [_Obj(query_length=8 * 64) for _ in range(3)]
     e.dc, e.sdc = DC(), SDC()
+    e.scan = _Obj()  # the native DB pass (irs_scan_*): configure / run are no-ops here
     e.threshold_a, e.max_variants, e.max_reauth, e.db_len = 16384, 16, 8, 4096
     e._pin, e._pinned, e._events, e._inflight, e._par = None, [], None, [None, None], 0
     e.graphs, e.tuned, e.autotune, e.tune_log, e.fixed = {}, {}, False, {}, None
