@@ -222,6 +222,9 @@ def test_plain_scan_every_candidate(dm, oracle, data):
         dm.synchronize()
         got = irisb200.bitmap_get(dc.fetch_bitmap(N_Q, N_DB), N_Q, N_DB)
         assert np.array_equal(got, exp), f"tuned {best}"
+        # restricted to one path: only that path's candidates are timed
+        only = ps.tune(only_path="fused")
+        assert only[0] == "fused" and {cd[0] for cd, _ in ps.tune_log} == {"fused"}
         ps.restore()
         ps.close()
     finally:
