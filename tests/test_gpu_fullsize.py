@@ -1,7 +1,8 @@
 """Parity at the benchmark's full size: 64 queries x 31 rotations against
 524,288 share-DB entries per party (3 parties, 60 GB resident).  The whole DB
-is scanned in one chunk and again in four chunks; the bitmaps must be equal
-(chunking invariance), every planted near-duplicate must be found, and the
+is scanned in one chunk, in four chunks and by the library's native pass as
+tuned on the batch; the bitmaps must be equal (chunking invariance, every
+path), every planted near-duplicate must be found, and the
 CPU path on the same shares (records read back from the device) must agree
 on blocks of entries at the start, the end and around the planted entries
 and on a strided sample of 4,096 entries spread over the whole DB (one entry
@@ -50,6 +51,20 @@ def test_full_size_parity(dm, oracle):
         dm.synchronize()
         bm = [irisb200.bitmap_get(dc.fetch_bitmap(NQ, M), NQ, M) for dc in dcs]
         assert np.array_equal(bm[0], bm[1]), "one chunk and four chunks differ"
+        # the library's native pass, as the benchmark runs it: tuned on this
+        # batch (a single timing pass per candidate), then one pass on dcs[1]
+        from irisb200.scan import PlainScan
+        ps = PlainScan(dm, ce, me, c, dcs[1], NQ, M, A)
+        try:
+            best = ps.tune(passes=1, finalists=2, rounds=1)
+            dcs[1].reset()
+            ps.scan()
+            dm.synchronize()
+            tuned = irisb200.bitmap_get(dcs[1].fetch_bitmap(NQ, M), NQ, M)
+            assert np.array_equal(tuned, bm[0]), f"the tuned native pass ({best}) differs"
+        finally:
+            ps.restore()
+            ps.close()
         got = bm[0]
         for j, (e, _) in planted.items():
             assert got[j, e], f"planted query {j} -> {e} not found"
