@@ -137,3 +137,35 @@ def test_bit_transposes(harness):
     for r in range(32):
         exp = sum(((int(a[c]) >> r) & 1) << c for c in range(32))
         assert int(t[r]) == exp
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the header's structs have the C sizes and field
+    offsets (compiled against include/irisb200.h with the host compiler)."""
+    import irisb200
+    src = tmp_path / "layout.c"
+    src.write_text("""
+#include <stddef.h>
+#include <stdio.h>
+#include "irisb200.h"
+#define F(T, m) printf(#T "." #m " %zu\\n", offsetof(T, m))
+int main(void) {
+  printf("irs_query_slot %zu\\n", sizeof(irs_query_slot));
+  F(irs_query_slot, src); F(irs_query_slot, rot_lo); F(irs_query_slot, n_rot); F(irs_query_slot, query);
+  printf("irs_scan_candidate %zu\\n", sizeof(irs_scan_candidate));
+  F(irs_scan_candidate, path); F(irs_scan_candidate, tile); F(irs_scan_candidate, chunk);
+  printf("irs_scan_timing %zu\\n", sizeof(irs_scan_timing));
+  F(irs_scan_timing, cand); F(irs_scan_timing, ms); F(irs_scan_timing, finalist); F(irs_scan_timing, reserved);
+  return 0;
+}
+""")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                               check=True).stdout.split("\n") if line)
+    mirrors = {"irs_query_slot": irisb200.QuerySlot, "irs_scan_candidate": irisb200.ScanCandidate,
+               "irs_scan_timing": irisb200.ScanTiming}
+    for cname, cls in mirrors.items():
+        assert int(got[cname]) == C.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert int(got[f"{cname}.{field}"]) == getattr(cls, field).offset, f"{cname}.{field}"
